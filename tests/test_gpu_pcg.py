@@ -1,0 +1,237 @@
+"""GPU parity tests through the C ABI against the CPU oracle.
+
+Bars:
+* WSB_PREC_REFERENCE_F32 (the reference's arithmetic): bit-identical x,
+  iteration count and residual history to the oracle's restatement of
+  compute.rs:189-495.
+* The fused FP64-reduction path: iteration count within 2% of the FP32
+  oracle and solution within 1e-5 relative (L2) of it on the synthetic
+  lattices; on the reference datasets (cond 1e10-1e12, where any change of
+  reduction order moves the FP32 iterates) within 2% or 2 iterations and
+  within the larger of 1e-5 and twice the oracle's own distance to x_ref;
+  exact iteration count against the oracle variant with FP64 dot products.
+* Every dataset result passes the reference's compare-x gate.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import wgpu_solver_backend_b200 as wsb
+from conftest import COMPARE_X_GATES, DATASET_SOLVE, load_case
+
+pytestmark = pytest.mark.gpu
+
+REL_X_TOL = 1e-5       # solution vs FP32 oracle, relative L2
+ITER_TOL = 0.02        # iteration count vs FP32 oracle
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a.astype(np.float64) - b.astype(np.float64)) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("k", [1, 2, 3])
+def test_reference_mode_bit_exact_on_datasets(ctx, k):
+    case, x_ref, fx = load_case(k)
+    a = case.a
+    m = wsb.Matrix.create(ctx, a.row_ptr, a.col_idx, a.values, case.block_starts, layout=wsb.LAYOUT_CSR)
+    x, res = m.solve(case.b, case.x0, precision=wsb.PREC_REFERENCE_F32, history_capacity=2000, **DATASET_SOLVE)
+    assert res["iterations"] == int(fx["iterations"])
+    assert np.array_equal(x.view(np.uint32), fx["x"].view(np.uint32))
+    assert np.array_equal(res["history"].astype(np.float32).view(np.uint32), fx["history"].view(np.uint32))
+
+
+@pytest.mark.parametrize("k", [1, 2, 3])
+def test_reference_api_executor_path_matches(ctx, k):
+    """pcg_block_jacobi_csr_wgpu with the five executors, as run_pcg_case
+    (cli main.rs:477-558) wires them."""
+    case, x_ref, fx = load_case(k)
+    a = case.a
+    n = a.n_rows
+    spmv = wsb.SpmvExecutor.create(ctx, n, a.row_ptr, a.col_idx, a.values)
+    vec = wsb.VecOpsExecutor.create(ctx)
+    dot = wsb.DotScalarExecutor.create(ctx, n, 7)
+    lu = wsb.build_lu_blocks_from_csr_block_starts_6(n, a.row_ptr, a.col_idx, a.values, case.block_starts)
+    bj = wsb.BlockJacobiExecutor.create(ctx, n, lu, case.block_starts)
+    up = wsb.PcgUpdateScalarsExecutor.create(ctx)
+    x = case.x0.copy()
+    it = wsb.pcg_block_jacobi_csr_wgpu(n, case.b, x, DATASET_SOLVE["max_iter"], DATASET_SOLVE["rel_tol"],
+                                       DATASET_SOLVE["abs_tol"], ctx, spmv, vec, dot, bj, up,
+                                       precision=wsb.PREC_REFERENCE_F32)
+    assert it == int(fx["iterations"]) and np.array_equal(x.view(np.uint32), fx["x"].view(np.uint32))
+    # Default (fused) precision through the same entry point.
+    x2 = case.x0.copy()
+    it2 = wsb.pcg_block_jacobi_csr_wgpu(n, case.b, x2, DATASET_SOLVE["max_iter"], DATASET_SOLVE["rel_tol"],
+                                        DATASET_SOLVE["abs_tol"], ctx, spmv, vec, dot, bj, up)
+    assert abs(it2 - it) <= max(2, ITER_TOL * it)
+    cmp = oracle.compare_x(x_ref, x2)
+    rt, at = COMPARE_X_GATES[k]
+    assert cmp["rel_l2"] <= rt or cmp["rmse"] <= at
+
+
+@pytest.mark.parametrize("k", [1, 2, 3])
+def test_fused_path_parity_on_datasets(ctx, k):
+    case, x_ref, fx = load_case(k)
+    a = case.a
+    m = wsb.Matrix.create(ctx, a.row_ptr, a.col_idx, a.values, case.block_starts)
+    x, res = m.solve(case.b, case.x0, **DATASET_SOLVE)
+    it_ref = int(fx["iterations"])
+    assert abs(res["iterations"] - it_ref) <= max(2, ITER_TOL * it_ref), (res["iterations"], it_ref)
+    f64 = oracle.pcg_f64dot(a.row_ptr, a.col_idx, a.values, fx["lu"], case.block_starts, case.b, case.x0,
+                            **{"max_iter": 2000, "rel_tol": 1e-4, "abs_tol": 1e-7})
+    assert abs(res["iterations"] - f64["iterations"]) <= 1
+    cmp = oracle.compare_x(x_ref, x)
+    rt, at = COMPARE_X_GATES[k]
+    assert cmp["rel_l2"] <= rt or cmp["rmse"] <= at, cmp
+    # Solution agreement with the FP32 oracle; on these ill-conditioned
+    # systems (cond 1e10-1e12) the bar is the oracle's own distance to x_ref.
+    d = rel(x, fx["x"])
+    assert d <= max(REL_X_TOL, 2.0 * rel(fx["x"], x_ref)), d
+
+
+@pytest.mark.parametrize("layout", [wsb.LAYOUT_CSR, wsb.LAYOUT_BSR6])
+def test_fused_path_parity_on_lattice(ctx, layout):
+    s = wsb.lattice_generate(10, seed=1)
+    n = s["n"]
+    m = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], layout=layout)
+    assert m.info["layout"] == layout
+    x, res = m.solve(s["b"], max_iter=5000, rel_tol=1e-6, history_capacity=5000)
+    lu = wsb.build_lu_blocks_from_csr_block_starts_6(n, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"])
+    ref = oracle.pcg_ref_f32(s["row_ptr"], s["col_idx"], s["values"], lu, s["block_starts"], s["b"],
+                             np.zeros(n, np.float32), 5000, 1e-6, 0.0)
+    assert abs(res["iterations"] - ref["iterations"]) <= max(1, ITER_TOL * ref["iterations"])
+    assert rel(x, ref["x"]) < REL_X_TOL
+    f64 = oracle.pcg_f64dot(s["row_ptr"], s["col_idx"], s["values"], lu, s["block_starts"], s["b"],
+                            np.zeros(n, np.float32), 5000, 1e-6, 0.0)
+    assert res["iterations"] == f64["iterations"]
+    assert rel(x, f64["x"]) < 1e-6
+    np.testing.assert_allclose(res["history"], f64["history"], rtol=1e-6)
+
+
+def test_bsr6_and_csr_are_bit_identical(ctx):
+    s = wsb.lattice_generate(9, seed=5)
+    mc = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], layout=wsb.LAYOUT_CSR)
+    mb = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], layout=wsb.LAYOUT_BSR6)
+    xc, rc = mc.solve(s["b"], max_iter=3000, rel_tol=1e-7)
+    xb, rb = mb.solve(s["b"], max_iter=3000, rel_tol=1e-7)
+    assert rc["iterations"] == rb["iterations"]
+    assert np.array_equal(xc.view(np.uint32), xb.view(np.uint32))
+
+
+def test_determinism_and_repeat_solves(ctx):
+    s = wsb.lattice_generate(7, seed=9)
+    m = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"])
+    x1, r1 = m.solve(s["b"], max_iter=3000, rel_tol=1e-6)
+    x2, r2 = m.solve(s["b"], max_iter=3000, rel_tol=1e-6)
+    assert r1["iterations"] == r2["iterations"] and np.array_equal(x1, x2)
+    # A different right-hand side on the cached workspace.
+    b3 = (s["b"] * 0.5).astype(np.float32)
+    x3, _ = m.solve(b3, max_iter=3000, rel_tol=1e-6)
+    assert rel(x3, 0.5 * x1) < 1e-5
+
+
+def test_zero_rhs_returns_zero_iterations_and_keeps_x(ctx):
+    s = wsb.lattice_generate(3, seed=2)
+    m = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], layout=wsb.LAYOUT_CSR)
+    x0 = np.full(s["n"], 3.0, np.float32)
+    for prec in (wsb.PREC_F32_F64DOT, wsb.PREC_REFERENCE_F32):
+        x, res = m.solve(np.zeros(s["n"], np.float32), x0, max_iter=10, rel_tol=1e-6, precision=prec)
+        assert res["iterations"] == 0 and res["rc"] == 0
+        assert np.array_equal(x, x0)
+
+
+def test_max_iter_reports_not_converged_and_leaves_x(ctx):
+    s = wsb.lattice_generate(6, seed=4)
+    m = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], layout=wsb.LAYOUT_CSR)
+    x0 = np.zeros(s["n"], np.float32)
+    for prec in (wsb.PREC_F32_F64DOT, wsb.PREC_REFERENCE_F32):
+        with pytest.raises(wsb.WsbError) as e:
+            m.solve(s["b"], x0, max_iter=3, rel_tol=1e-12, precision=prec)
+        assert e.value.status == wsb._lib.NOT_CONVERGED
+        assert "did not converge in 3 iterations" in str(e.value)
+        x, res = m.solve(s["b"], x0, max_iter=3, rel_tol=1e-12, precision=prec, raise_on_error=False)
+        assert res["iterations"] == 3 and np.array_equal(x, x0)
+        x, res = m.solve(s["b"], x0, max_iter=0, rel_tol=1e-12, precision=prec, raise_on_error=False)
+        assert res["rc"] == wsb._lib.NOT_CONVERGED and res["iterations"] == 0
+
+
+def test_breakdown_pAp_zero(ctx):
+    # Indefinite diag(1, -1), 1x1 blocks, b = (1, 1): p = z = (1, -1), pAp = 0
+    # (compute.rs:473-475).
+    rp, ci, v, bs = [0, 1, 2], [0, 1], [1.0, -1.0], [0, 1, 2]
+    m = wsb.Matrix.create(ctx, rp, ci, v, bs, layout=wsb.LAYOUT_CSR)
+    for prec in (wsb.PREC_F32_F64DOT, wsb.PREC_REFERENCE_F32):
+        with pytest.raises(wsb.WsbError) as e:
+            m.solve(np.ones(2, np.float32), max_iter=10, rel_tol=1e-6, precision=prec)
+        assert e.value.status == wsb._lib.BREAKDOWN and "dot(p,Ap) is zero" in str(e.value)
+
+
+def test_zero_pivot_rejected_at_matrix_creation(ctx):
+    rp, ci, v = [0, 2, 4], [0, 1, 0, 1], [0.0, 1.0, 1.0, 0.0]
+    with pytest.raises(wsb.WsbError) as e:
+        wsb.Matrix.create(ctx, rp, ci, v, [0, 2])
+    assert e.value.status == wsb._lib.ZERO_PIVOT and "LU zero pivot at k = 0" in str(e.value)
+
+
+def _irregular(n_nodes=60, seed=0):
+    """A lattice matrix with an irregular block partition (1..9 rows)."""
+    s = wsb.lattice_generate(5, seed=seed)
+    n = s["n"]
+    rng = np.random.default_rng(seed)
+    cuts = [0]
+    while cuts[-1] < n:
+        cuts.append(min(n, cuts[-1] + int(rng.integers(1, 10))))
+    s["block_starts"] = np.array(cuts, np.uint32)
+    return s
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_irregular_blocks_including_longer_than_six(ctx, seed):
+    s = _irregular(seed=seed)
+    n = s["n"]
+    bs = s["block_starts"]
+    lu = wsb.build_lu_blocks_from_csr_block_starts_6(n, s["row_ptr"], s["col_idx"], s["values"], bs)
+    ref = oracle.pcg_ref_f32(s["row_ptr"], s["col_idx"], s["values"], lu, bs, s["b"], np.zeros(n, np.float32),
+                             4000, 1e-6, 0.0)
+    m = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], bs)
+    assert m.info["layout"] == wsb.LAYOUT_CSR
+    xr, rr = m.solve(s["b"], max_iter=4000, rel_tol=1e-6, precision=wsb.PREC_REFERENCE_F32, raise_on_error=False)
+    assert rr["rc"] == ref["status"] and rr["iterations"] == ref["iterations"]
+    assert np.array_equal(xr.view(np.uint32), ref["x"].view(np.uint32))
+    f64 = oracle.pcg_f64dot(s["row_ptr"], s["col_idx"], s["values"], lu, bs, s["b"], np.zeros(n, np.float32),
+                            4000, 1e-6, 0.0)
+    xf, rf = m.solve(s["b"], max_iter=4000, rel_tol=1e-6, raise_on_error=False)
+    assert rf["rc"] == f64["status"] and rf["iterations"] == f64["iterations"]
+    assert rel(xf, f64["x"]) < 1e-6
+
+
+def test_long_rows_are_chunked(ctx):
+    # Dense rows (n = 20000 nonzeros in row 0) exceed one shared-memory chunk.
+    n = 20000
+    rng = np.random.default_rng(3)
+    rows, cols, vals = [], [], []
+    rp = [0]
+    for i in range(n):
+        if i == 0:
+            c = np.arange(n)
+            vv = rng.uniform(-1e-3, 1e-3, n).astype(np.float32)
+            vv[0] = 50.0
+        else:
+            c = np.array(sorted({0, i}))
+            vv = np.array([1e-3, 4.0] if len(c) == 2 else [4.0], np.float32)
+        cols.append(c)
+        vals.append(vv)
+        rp.append(rp[-1] + len(c))
+    ci = np.concatenate(cols).astype(np.uint32)
+    v = np.concatenate(vals).astype(np.float32)
+    rp = np.array(rp, np.uint32)
+    x = rng.standard_normal(n).astype(np.float32)
+    ref = oracle.spmv(rp, ci, v, x)
+    m = wsb.Matrix.create(ctx, rp, ci, v, np.arange(0, n + 1, dtype=np.uint32))
+    import torch
+
+    dx = torch.from_numpy(x).cuda()
+    dy = torch.zeros(n, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    m.spmv_device(dx.data_ptr(), dy.data_ptr())
+    ctx.synchronize()
+    assert np.array_equal(dy.cpu().numpy().view(np.uint32), ref.view(np.uint32))

@@ -1,0 +1,39 @@
+// Fused PCG kernels for sm_100a (declarations shared with the engine).
+//
+// One PCG iteration of every active system is three launches:
+//   k_spmv     Ap = A p (CSR or BSR6 tiles streamed through shared memory with
+//              128-bit loads), FP64 p.Ap per tile, and in the last CTA of each
+//              system: pAp, alpha = rz_old / pAp.
+//   k_update   x += alpha p, r -= alpha Ap, z = (LU)^-1 r per 6x6 block in
+//              registers, FP64 r.r and r.z per tile; the last CTA of each system
+//              computes beta, the stop test, the residual history and status.
+//   k_pupdate  p = z + beta p; one thread of CTA 0 clears the graph's while
+//              condition when no system is left.
+// These replace the reference's 17 passes per iteration (compute.rs:336-489):
+// spmv.wgsl, dot_partials.wgsl + dot_reduce.wgsl (x3), pcg_update_scalars.wgsl
+// (x2), axpy*.wgsl (x3), scale_from_scalar_results.wgsl, block_jacobi.wgsl.
+#pragma once
+#include "wsb_internal.h"
+
+namespace wsb {
+
+// Bytes of dynamic shared memory used by k_spmv.
+constexpr size_t kSpmvSmem = (size_t)kCsrCap * sizeof(float) + (kTileRows + 8) * sizeof(uint32_t);
+
+// k_spmv_loop: Ap = A p with p.Ap and alpha; k_spmv_init: Ap = A x.
+__global__ void k_spmv_loop(const SysDesc *__restrict__ sys, StepParams *sp);
+__global__ void k_spmv_init(const SysDesc *__restrict__ sys, StepParams *sp);
+__global__ void k_update(const SysDesc *__restrict__ sys, StepParams *sp);
+__global__ void k_init(const SysDesc *__restrict__ sys, StepParams *sp);
+__global__ void k_pupdate(const SysDesc *__restrict__ sys, StepParams *sp, cudaGraphConditionalHandle h);
+__global__ void k_loop_gate(StepParams *sp, cudaGraphConditionalHandle h);
+
+// Mixed precision.
+__global__ void k_resid64(const SysDesc *__restrict__ sys, StepParams *sp);
+__global__ void k_refine(const SysDesc *__restrict__ sys, StepParams *sp);
+__global__ void k_x64_to_x32(const SysDesc *__restrict__ sys, StepParams *sp);
+
+// Plain y = A x of one system over its own tiles (no reduction).
+__global__ void k_spmv_plain(const SysDesc *__restrict__ sys, const float *__restrict__ x, float *__restrict__ y);
+
+}  // namespace wsb

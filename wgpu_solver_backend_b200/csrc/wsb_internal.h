@@ -1,0 +1,169 @@
+// Internal declarations shared by the host library (.cpp) and the kernels (.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <functional>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/wsb.h"
+
+namespace wsb {
+
+// ---------------------------------------------------------------------------
+// Launch geometry shared by host and device code.
+// ---------------------------------------------------------------------------
+constexpr int kThreads = 256;        // threads per CTA for every solver kernel
+constexpr int kTileRows = 256;       // rows (or block rows x 6) per tile, <= kThreads
+constexpr int kCsrCap = 12288;       // CSR nonzeros staged in shared memory per chunk
+constexpr int kBsrCapBlocks = 256;   // BSR 6x6 blocks staged per chunk (36 KiB of values)
+constexpr int kLuStage = 64;         // LU blocks staged in shared memory per pass
+constexpr int kPadElems = 64;        // tail padding of streamed arrays (elements)
+
+enum SysStatus : uint32_t {
+    ST_RUNNING = 0,
+    ST_CONVERGED = 1,
+    ST_BREAKDOWN = 2,
+    ST_MAXITER = 3,
+};
+
+enum Layout : uint32_t { LAYOUT_CSR = 1, LAYOUT_BSR6 = 2 };
+
+// Row tile of the SpMV: rows [row0, row1) (CSR) or block rows (BSR6).
+struct SpmvTile {
+    uint32_t row0, row1;
+};
+// Row tile of the update kernels; never cuts the first 6 rows of a block.
+// Blocks whose first row lies in [row0, row1) are [blk0, blk1).
+struct UpdTile {
+    uint32_t row0, row1, blk0, blk1;
+};
+struct WorkItem {
+    uint32_t sys, tile;
+};
+
+// Mutable per-system scalars; written only by the last CTA of a reduction.
+struct alignas(64) SysState {
+    double bb, rz_old, pap, rr, rz_new, alpha, beta;
+    double rel2, abs2;
+    float alpha_f, beta_f;
+    uint32_t iter, max_iter, status, active;
+    uint32_t cnt_a, cnt_b;      // last-CTA tickets of the two reductions
+    uint32_t breakdown;         // 1: pAp == 0, 2: rz_old == 0
+    uint32_t pad0;
+    double rr64, bb64;          // FP64 true residual and ||b||^2 (mixed precision)
+    uint32_t cnt_c, pad1;
+};
+
+// Read-mostly description of one system in device memory.
+struct SysDesc {
+    uint32_t n, nb, layout, hist_cap;
+    const uint32_t *row_ptr, *col;
+    const float *val;
+    const uint32_t *brow_ptr, *bcol;   // BSR6: block rows = n/6
+    const float *bval;                 // 36 floats per block, row-major
+    const float *lu;                   // 36 floats per diagonal block
+    const uint32_t *bstart;            // nb + 1
+    const float *b;                    // right-hand side of the (inner) PCG
+    float *x, *r, *z, *p, *ap;
+    const float *b_orig;               // mixed precision: the caller's b
+    double *x64;                       // mixed precision: FP64 solution
+    const SpmvTile *stiles;
+    const UpdTile *utiles;
+    uint32_t n_stiles, n_utiles;
+    double *part_a;                    // n_stiles partials
+    double2 *part_b;                   // n_utiles partial pairs
+    SysState *st;
+    double *history;                   // hist_cap entries or null
+};
+
+// Kernel parameters of one loop step that the host may change between graph
+// launches (work lists, counts); lives in device memory so a captured graph
+// stays valid.
+struct StepParams {
+    const WorkItem *work_a;            // loop: SpMV tiles of active systems
+    const WorkItem *work_b;            // loop: update tiles of active systems
+    const WorkItem *init_a;            // init: SpMV tiles of systems (re)starting
+    const WorkItem *init_b;            // init: update tiles of systems (re)starting
+    const WorkItem *aux_b;             // refinement kernels: update tiles
+    uint32_t n_work_a, n_work_b;
+    uint32_t n_init_a, n_init_b;
+    uint32_t n_aux_b;
+    uint32_t num_active;               // systems still iterating
+    uint32_t loop_count;               // body executions in this launch
+    uint32_t loop_limit;               // stop the while loop after this many
+};
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+void set_thread_error(const std::string &msg);
+const char *thread_error();
+
+struct Context;
+int fail(Context *ctx, int status, const char *fmt, ...);
+
+#define WSB_CUDA_TRY(ctx, expr)                                                              \
+    do {                                                                                     \
+        cudaError_t _e = (expr);                                                             \
+        if (_e != cudaSuccess)                                                               \
+            return ::wsb::fail((ctx), _e == cudaErrorMemoryAllocation ? WSB_ERR_OUT_OF_MEMORY \
+                                                                      : WSB_ERR_CUDA,          \
+                               "%s failed: %s (%s:%d)", #expr, cudaGetErrorString(_e),       \
+                               __FILE__, __LINE__);                                          \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+struct Context {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;     // own_stream or the caller's
+    cudaDeviceProp prop{};
+    int sm_count = 0;
+    std::string last_error;
+    std::mutex mu;
+};
+
+struct Buffer {
+    Context *ctx = nullptr;
+    void *ptr = nullptr;
+    size_t bytes = 0;
+};
+
+// Device allocation helper (zero-filled, padded).
+int dev_alloc(Context *ctx, void **p, size_t bytes, bool zero = true);
+void dev_free(void *p);
+
+// ---------------------------------------------------------------------------
+// Host-side setup helpers (lu.cpp, tiles.cpp)
+// ---------------------------------------------------------------------------
+int lu_factor_inplace_6(float *mat, uint32_t n, uint32_t *pivot_k);
+// Returns WSB_OK / WSB_ERR_BAD_INPUT / WSB_ERR_ZERO_PIVOT with message in *err.
+int build_lu_blocks_6(uint32_t n, const uint32_t *row_ptr, uint64_t row_ptr_len, const uint32_t *col,
+                      uint64_t col_len, const float *val, uint64_t val_len, const uint32_t *bs,
+                      uint64_t bs_len, float *out, std::string *err);
+// Validation of a CSR matrix + block partition (loaders.rs:44-212 rules).
+int validate_system(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, uint64_t nnz,
+                    const uint32_t *bs, uint64_t bs_len, std::string *err);
+
+void build_spmv_tiles_csr(uint32_t n, const uint32_t *row_ptr, std::vector<SpmvTile> *out);
+void build_spmv_tiles_bsr(uint32_t nbrows, const uint32_t *brow_ptr, std::vector<SpmvTile> *out);
+void build_upd_tiles(uint32_t n, const uint32_t *bs, uint32_t nb, std::vector<UpdTile> *out);
+// True when every block has 6 rows and every touched 6x6 block is fully stored.
+bool bsr6_convertible(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, const uint32_t *bs,
+                      uint64_t bs_len);
+// CSR -> BSR6 (requires bsr6_convertible). Returns block count.
+uint64_t csr_to_bsr6(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, const float *val,
+                     std::vector<uint32_t> *brow_ptr, std::vector<uint32_t> *bcol, std::vector<float> *bval);
+
+void parallel_for(int64_t n, int64_t grain, const std::function<void(int64_t, int64_t)> &fn);
+
+}  // namespace wsb
