@@ -147,7 +147,9 @@ def run_plain(args, world, rank, local):
 
     torch.cuda.set_device(local)
     ctx = wsb.GpuContext.create("auto", local)
-    stream = torch.cuda.current_stream()
+    # A dedicated (non-default) stream shared by torch events and the library.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     s = wsb.lattice_generate(PLAIN["side"], seed=PLAIN["seed"])
     n = s["n"]
@@ -175,21 +177,16 @@ def run_plain(args, world, rank, local):
     dev_s = e0.elapsed_time(e1) / 1e3
     dev_s = reduce_max(dev_s, world)
     barrier(world)
-    # SpMV kernel roofline: the tile SpMV of the matrix's layout, timed alone.
-    d_y = torch.empty(n, dtype=torch.float32, device="cuda")
-    for _ in range(3):
-        m.spmv_device(d_x.data_ptr(), d_y.data_ptr())
-    reps = 50
-    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e2.record(stream)
-    for _ in range(reps):
-        m.spmv_device(d_x.data_ptr(), d_y.data_ptr())
-    e3.record(stream)
-    torch.cuda.synchronize()
-    spmv_s = e2.elapsed_time(e3) / 1e3 / reps
+    # Per-kernel device times of the solver's own loop kernels (CUDA events
+    # around each launch, outside the graph), on the same matrix.
+    kt = m.kernel_times(d_b.data_ptr(), iterations=20)
+    spmv_s = kt["spmv_ms"] / 1e3
     peak, peak_kind = peaks()
     spmv_gbs = info["spmv_bytes"] / spmv_s / 1e9
+    upd_bytes = 28 * n + 144 * info["num_blocks"]
+    kernels = {"spmv": {"ms": kt["spmv_ms"], "bytes": info["spmv_bytes"], "gbs": spmv_gbs},
+               "update": {"ms": kt["update_ms"], "bytes": upd_bytes, "gbs": upd_bytes / kt["update_ms"] / 1e6},
+               "pupdate": {"ms": kt["pupdate_ms"], "bytes": 12 * n, "gbs": 12 * n / kt["pupdate_ms"] / 1e6}}
     iter_gbs = info["iteration_bytes"] * iters / (dev_s / args.steps) / 1e9
     # End to end through the C ABI with host buffers (copies in the timed region).
     x_host = np.zeros(n, np.float32)
@@ -214,7 +211,7 @@ def run_plain(args, world, rank, local):
                      "achieved": spmv_gbs, "peak": peak, "unit": "GB/s", "frac": spmv_gbs / peak,
                      "peak_kind": peak_kind, "traffic": None,
                      "algorithmic_bytes_per_launch": info["spmv_bytes"], "launch_us": spmv_s * 1e6},
-        "iteration_gbs": iter_gbs, "iteration_frac": iter_gbs / peak,
+        "iteration_gbs": iter_gbs, "iteration_frac": iter_gbs / peak, "kernels": kernels,
         "gpu_launches": args.steps * (2 + 1 + 3 * iters),
         "clocks": clk,
     }
@@ -252,14 +249,47 @@ def run_reference_plain(args, world, rank, local):
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_kernels(args, world, rank, local):
+    """Per-kernel device times of the three loop kernels on one lattice system
+    (the small case used for profiler captures)."""
+    import torch
+
+    import wgpu_solver_backend_b200 as wsb
+
+    torch.cuda.set_device(local)
+    ctx = wsb.GpuContext.create("auto", local)
+    s = wsb.lattice_generate(args.side, seed=PLAIN["seed"])
+    m = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"],
+                          layout=wsb.LAYOUT_CSR if args.layout == "csr" else wsb.LAYOUT_AUTO)
+    d_b = torch.from_numpy(s["b"]).cuda()
+    torch.cuda.synchronize()
+    kt = m.kernel_times(d_b.data_ptr(), iterations=args.iters)
+    info = m.info
+    peak, kind = peaks()
+    out = {"workload": f"kernels: {args.side}^3 lattice, n={s['n']}, layout {args.layout}", "iterations": args.iters,
+           "matrix_bytes": info["device_bytes"]}
+    for k, b in (("spmv", info["spmv_bytes"]), ("update", 28 * s["n"] + 144 * info["num_blocks"]),
+                 ("pupdate", 12 * s["n"])):
+        ms = kt[k + "_ms"]
+        out[k] = {"us": ms * 1e3, "bytes": b, "gbs": b / ms / 1e6, "frac": b / ms / 1e6 / peak}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="plain80", choices=["plain80"])
+    ap.add_argument("--workload", default="plain80", choices=["plain80", "kernels"])
+    ap.add_argument("--side", type=int, default=56, help="kernels workload: lattice side")
+    ap.add_argument("--iters", type=int, default=5, help="kernels workload: timed iterations")
+    ap.add_argument("--layout", default="auto", choices=["auto", "csr"])
     args = ap.parse_args()
+    if args.workload == "kernels":
+        world, rank, local = dist_setup()
+        print(json.dumps(run_kernels(args, world, rank, local)), flush=True)
+        return
     world, rank, local = dist_setup()
     if args.impl == "reference":
         if rank != 0:

@@ -246,6 +246,13 @@ int wsb_solve_device(wsb_context *ctx, wsb_matrix *m, const float *d_b, float *d
 /* y = A x with the product SpMV kernel of the matrix's layout (device pointers). */
 int wsb_matrix_spmv_device(wsb_context *ctx, wsb_matrix *m, const float *d_x, float *d_y);
 
+/* Measurement aid (no counterpart in the reference): runs `iterations` PCG
+ * iterations of this matrix with right-hand side d_b (device) outside the
+ * CUDA graph, CUDA events around each launch, and writes the mean duration
+ * in ms of the SpMV+p.Ap kernel, the update+preconditioner kernel and the
+ * p-update kernel to ms[0..2]. */
+int wsb_matrix_kernel_times(wsb_context *ctx, wsb_matrix *m, const float *d_b, uint32_t iterations, double *ms);
+
 /* ------------------------------------------------------------------------- */
 /* Batched solve of many independent systems                                 */
 /* ------------------------------------------------------------------------- */

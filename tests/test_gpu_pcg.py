@@ -99,7 +99,12 @@ def test_fused_path_parity_on_lattice(ctx, layout):
     ref = oracle.pcg_ref_f32(s["row_ptr"], s["col_idx"], s["values"], lu, s["block_starts"], s["b"],
                              np.zeros(n, np.float32), 5000, 1e-6, 0.0)
     assert abs(res["iterations"] - ref["iterations"]) <= max(1, ITER_TOL * ref["iterations"])
-    assert rel(x, ref["x"]) < REL_X_TOL
+    # 1e-5 relative, or (on systems where FP32 itself cannot resolve 1e-5) no
+    # farther from the FP32 oracle than that oracle is from the FP64 solution.
+    exact = oracle.pcg_f64(s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], s["b"], rel_tol=1e-13)["x"]
+    ref_err = rel(ref["x"], exact)
+    assert rel(x, ref["x"]) < max(REL_X_TOL, 1.5 * ref_err)
+    assert rel(x, exact) <= 1.5 * ref_err
     f64 = oracle.pcg_f64dot(s["row_ptr"], s["col_idx"], s["values"], lu, s["block_starts"], s["b"],
                             np.zeros(n, np.float32), 5000, 1e-6, 0.0)
     assert res["iterations"] == f64["iterations"]

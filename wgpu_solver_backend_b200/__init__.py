@@ -402,6 +402,13 @@ class Matrix:
             _check(rc, self.ctx.handle)
         return out
 
+    def kernel_times(self, d_b: int, iterations: int = 20) -> dict:
+        """Mean per-launch device time (ms) of the three loop kernels."""
+        ms = np.zeros(3, np.float64)
+        _check(_lib_handle().wsb_matrix_kernel_times(self.ctx.handle, self.handle, C.c_void_p(d_b), int(iterations),
+                                                     _p(ms, _lib.f64p)), self.ctx.handle)
+        return dict(spmv_ms=ms[0], update_ms=ms[1], pupdate_ms=ms[2])
+
     def spmv_device(self, d_x: int, d_y: int):
         _check(_lib_handle().wsb_matrix_spmv_device(self.ctx.handle, self.handle, C.c_void_p(d_x), C.c_void_p(d_y)),
                self.ctx.handle)

@@ -108,6 +108,7 @@ SIGNATURES = {
     "wsb_solve_device": (C.c_int, [vp, vp, vp, vp, C.c_uint64, C.c_float, C.c_float, C.POINTER(SolveOpts),
                                    C.POINTER(SolveResult)]),
     "wsb_matrix_spmv_device": (C.c_int, [vp, vp, vp, vp]),
+    "wsb_matrix_kernel_times": (C.c_int, [vp, vp, vp, C.c_uint32, f64p]),
     "wsb_batch_create": (C.c_int, [vp, C.POINTER(vp)]),
     "wsb_batch_add": (C.c_int, [vp, vp, f32p, f32p, C.c_uint64, C.c_float, C.c_float, C.POINTER(SolveOpts),
                                 C.POINTER(C.c_uint32)]),

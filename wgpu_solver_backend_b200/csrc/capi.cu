@@ -799,20 +799,46 @@ extern "C" int wsb_matrix_spmv_device(wsb_context *ctx, wsb_matrix *m, const flo
     d.bval = m->A.bval;
     d.stiles = m->A.stiles;
     d.n_stiles = m->A.n_stiles;
-    static thread_local SysDesc *dd = nullptr;
-    static thread_local int dd_dev = -1;
-    if (!dd || dd_dev != ctx->device) {
-        WSB_CUDA_TRY(ctx, cudaMalloc(&dd, sizeof(SysDesc)));
-        dd_dev = ctx->device;
+    // Per-thread, per-device scratch for the descriptor and the error word.
+    struct Scratch {
+        SysDesc *dd = nullptr;
+        StepParams *sp = nullptr;
+        int dev = -1;
+    };
+    static thread_local Scratch sc;
+    if (!sc.dd || sc.dev != ctx->device) {
+        WSB_CUDA_TRY(ctx, cudaMalloc(&sc.dd, sizeof(SysDesc)));
+        WSB_CUDA_TRY(ctx, cudaMalloc(&sc.sp, sizeof(StepParams)));
+        WSB_CUDA_TRY(ctx, cudaMemset(sc.sp, 0, sizeof(StepParams)));
+        sc.dev = ctx->device;
         cudaFuncSetAttribute(k_spmv_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpmvSmem);
     }
-    WSB_CUDA_TRY(ctx, cudaMemcpyAsync(dd, &d, sizeof d, cudaMemcpyHostToDevice, ctx->stream));
+    WSB_CUDA_TRY(ctx, cudaMemcpyAsync(sc.dd, &d, sizeof d, cudaMemcpyHostToDevice, ctx->stream));
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_spmv_plain, kThreads, kSpmvSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_spmv_plain, kPipeThreads, kSpmvSmem);
     const uint32_t g = std::max<uint32_t>(1, std::min<uint32_t>(m->A.n_stiles, (uint32_t)(std::max(occ, 1) * ctx->sm_count)));
-    k_spmv_plain<<<g, kThreads, kSpmvSmem, ctx->stream>>>(dd, d_x, d_y);
+    k_spmv_plain<<<g, kPipeThreads, kSpmvSmem, ctx->stream>>>(sc.dd, sc.sp, d_x, d_y);
     WSB_CUDA_TRY(ctx, cudaGetLastError());
     return WSB_OK;
+}
+
+extern "C" int wsb_matrix_kernel_times(wsb_context *ctx, wsb_matrix *m, const float *d_b, uint32_t iterations,
+                                       double *ms) {
+    CHECK_CTX(ctx);
+    if (!m || !d_b || !ms || iterations == 0) return fail(ctx, WSB_ERR_BAD_INPUT, "bad arguments");
+    Engine E(ctx, ctx->stream);
+    SolveCfg cfg;
+    cfg.max_iter = iterations + 1;
+    uint32_t slot;
+    int rc = E.add(&m->A, &m->M, cfg, &slot);
+    if (rc) return rc;
+    float *d_x0 = nullptr;
+    WSB_CUDA_TRY(ctx, cudaMallocAsync((void **)&d_x0, sizeof(float) * std::max<uint32_t>(m->A.n, 1), ctx->stream));
+    WSB_CUDA_TRY(ctx, cudaMemsetAsync(d_x0, 0, sizeof(float) * std::max<uint32_t>(m->A.n, 1), ctx->stream));
+    rc = E.set_rhs(slot, d_b, d_x0, true);
+    if (!rc) rc = E.profile_kernels(slot, iterations, ms);
+    cudaFreeAsync(d_x0, ctx->stream);
+    return rc;
 }
 
 // ---------------------------------------------------------------------------

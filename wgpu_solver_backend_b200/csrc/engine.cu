@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "engine.h"
@@ -56,9 +57,9 @@ int upload_matA(Context *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_
         std::vector<float> bval;
         out->nbsr = csr_to_bsr6(n, row_ptr, col, val, &brow_ptr, &bcol, &bval);
         out->layout = LAYOUT_BSR6;
-        if ((rc = upload(ctx, &out->brow_ptr, brow_ptr.data(), brow_ptr.size(), 0, st, &out->bytes))) return rc;
+        if ((rc = upload(ctx, &out->brow_ptr, brow_ptr.data(), brow_ptr.size(), 8, st, &out->bytes))) return rc;
         if ((rc = upload(ctx, &out->bcol, bcol.data(), bcol.size(), kPadElems, st, &out->bytes))) return rc;
-        if ((rc = upload(ctx, &out->bval, bval.data(), bval.size(), 0, st, &out->bytes))) return rc;
+        if ((rc = upload(ctx, &out->bval, bval.data(), bval.size(), 16, st, &out->bytes))) return rc;
         std::vector<SpmvTile> tiles;
         build_spmv_tiles_bsr(n / 6, brow_ptr.data(), &tiles);
         out->n_stiles = (uint32_t)tiles.size();
@@ -67,7 +68,7 @@ int upload_matA(Context *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_
         return WSB_OK;
     }
     out->layout = LAYOUT_CSR;
-    if ((rc = upload(ctx, &out->row_ptr, row_ptr, (size_t)n + 1, 0, st, &out->bytes))) return rc;
+    if ((rc = upload(ctx, &out->row_ptr, row_ptr, (size_t)n + 1, 8, st, &out->bytes))) return rc;
     if ((rc = upload(ctx, &out->col, col, nnz, kPadElems, st, &out->bytes))) return rc;
     if ((rc = upload(ctx, &out->val, val, nnz, kPadElems, st, &out->bytes))) return rc;
     std::vector<SpmvTile> tiles;
@@ -85,7 +86,7 @@ int upload_precond(Context *ctx, uint32_t n, const float *lu, const uint32_t *bs
     out->nb = bs_len >= 1 ? (uint32_t)(bs_len - 1) : 0;
     int rc;
     if ((rc = upload(ctx, &out->lu, lu, (size_t)out->nb * 36, 4, st, &out->bytes))) return rc;
-    if ((rc = upload(ctx, &out->bs, bs, (size_t)bs_len, 1, st, &out->bytes))) return rc;
+    if ((rc = upload(ctx, &out->bs, bs, (size_t)bs_len, 8, st, &out->bytes))) return rc;
     std::vector<UpdTile> tiles;
     build_upd_tiles(n, bs, out->nb, &tiles);
     out->n_utiles = (uint32_t)tiles.size();
@@ -135,11 +136,17 @@ Engine::Engine(Context *ctx, cudaStream_t stream) : ctx_(ctx), stream_(stream) {
     cudaFuncSetAttribute(k_spmv_loop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpmvSmem);
     cudaFuncSetAttribute(k_spmv_init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpmvSmem);
     cudaFuncSetAttribute(k_spmv_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpmvSmem);
-    int occ_a = 0, occ_b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_spmv_loop, kThreads, kSpmvSmem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_update, kThreads, 0);
+    cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdSmem);
+    cudaFuncSetAttribute(k_init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdSmem);
+    int occ_a = 0, occ_b = 0, occ_c = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_spmv_loop, kPipeThreads, kSpmvSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_update, kPipeThreads, kUpdSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_pupdate, kThreads, 0);
     max_grid_a_ = std::max(1, occ_a) * std::max(1, ctx->sm_count);
     max_grid_b_ = std::max(1, occ_b) * std::max(1, ctx->sm_count);
+    max_grid_c_ = std::max(1, occ_c) * std::max(1, ctx->sm_count);
+    const char *loop_env = getenv("WSB_LOOP");
+    use_graph_ = !(loop_env && std::strcmp(loop_env, "launch") == 0);
     cudaMallocHost(&h_sp_, sizeof(StepParams));
     cudaMallocHost(&h_sp_rb_, sizeof(StepParams));
     std::memset(h_sp_, 0, sizeof(StepParams));
@@ -203,7 +210,7 @@ int Engine::ensure_capacity(uint32_t need) {
     if (graph_) cudaGraphDestroy(graph_);
     exec_ = nullptr;
     graph_ = nullptr;
-    graph_grid_a_ = graph_grid_b_ = 0;
+    graph_grid_a_ = graph_grid_b_ = graph_grid_c_ = 0;
     return WSB_OK;
 }
 
@@ -359,7 +366,7 @@ void Engine::remove(uint32_t s) {
     std::memset(h_sys_ + s, 0, sizeof(SysDesc));
 }
 
-// Work-list storage: five lists (loop a/b, init a/b, aux b) of work_cap_
+// Work-list storage: six lists (loop a/b/c, init a/b, aux b) of work_cap_
 // items each, in one device array with a pinned host mirror. The host only
 // rewrites a region before the copy that feeds the next kernel reading it, so
 // a copy still pending from earlier in the same step carries either the same
@@ -367,7 +374,7 @@ void Engine::remove(uint32_t s) {
 int Engine::rebuild_work() {
     size_t per = 1;
     for (auto &s : slots_)
-        if (s) per += std::max(s->A->n_stiles, s->M->n_utiles);
+        if (s) per += std::max<size_t>(std::max(s->A->n_stiles, s->M->n_utiles), chunks_of(s->A->n));
     if (per > work_cap_) {
         WSB_CUDA_TRY(ctx_, cudaStreamSynchronize(stream_));
         const size_t nc = std::max(per, work_cap_ * 2);
@@ -375,28 +382,40 @@ int Engine::rebuild_work() {
         cudaFreeHost(h_work_);
         d_work_ = nullptr;
         h_work_ = nullptr;
-        WSB_CUDA_TRY(ctx_, cudaMalloc(&d_work_, sizeof(WorkItem) * nc * 5));
-        WSB_CUDA_TRY(ctx_, cudaMallocHost(&h_work_, sizeof(WorkItem) * nc * 5));
+        WSB_CUDA_TRY(ctx_, cudaMalloc(&d_work_, sizeof(WorkItem) * nc * kLists));
+        WSB_CUDA_TRY(ctx_, cudaMallocHost(&h_work_, sizeof(WorkItem) * nc * kLists));
         work_cap_ = nc;
     }
-    uint32_t na = 0, nb = 0;
-    WorkItem *wa = h_work_, *wb = h_work_ + work_cap_;
+    uint32_t na = 0, nb = 0, nch = 0;
+    WorkItem *wa = h_work_ + L_A * work_cap_, *wb = h_work_ + L_B * work_cap_, *wc = h_work_ + L_C * work_cap_;
     for (uint32_t s = 0; s < slots_.size(); ++s) {
         const Slot *sl = slots_[s].get();
         if (!sl || sl->phase != Slot::RUNNING) continue;
         for (uint32_t t = 0; t < sl->A->n_stiles; ++t) wa[na++] = {s, t};
         for (uint32_t t = 0; t < sl->M->n_utiles; ++t) wb[nb++] = {s, t};
+        for (uint32_t t = 0; t < chunks_of(sl->A->n); ++t) wc[nch++] = {s, t};
     }
     n_work_a_ = na;
     n_work_b_ = nb;
-    if (na) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_, wa, sizeof(WorkItem) * na, cudaMemcpyHostToDevice, stream_));
-    if (nb)
-        WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + work_cap_, wb, sizeof(WorkItem) * nb, cudaMemcpyHostToDevice, stream_));
+    n_work_c_ = nch;
+    if (na) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + L_A * work_cap_, wa, sizeof(WorkItem) * na, cudaMemcpyHostToDevice, stream_));
+    if (nb) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + L_B * work_cap_, wb, sizeof(WorkItem) * nb, cudaMemcpyHostToDevice, stream_));
+    if (nch) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + L_C * work_cap_, wc, sizeof(WorkItem) * nch, cudaMemcpyHostToDevice, stream_));
     work_dirty_ = false;
     return WSB_OK;
 }
 
-int Engine::capture_loop(uint32_t ga, uint32_t gb) {
+void Engine::fill_list_ptrs() {
+    h_sp_->num_sys = cap_;
+    h_sp_->work_a = d_work_ + L_A * work_cap_;
+    h_sp_->work_b = d_work_ + L_B * work_cap_;
+    h_sp_->work_c = d_work_ + L_C * work_cap_;
+    h_sp_->init_a = d_work_ + L_IA * work_cap_;
+    h_sp_->init_b = d_work_ + L_IB * work_cap_;
+    h_sp_->aux_b = d_work_ + L_X * work_cap_;
+}
+
+int Engine::capture_loop(uint32_t ga, uint32_t gb, uint32_t gc) {
     if (exec_) cudaGraphExecDestroy(exec_);
     if (graph_) cudaGraphDestroy(graph_);
     exec_ = nullptr;
@@ -425,9 +444,9 @@ int Engine::capture_loop(uint32_t ga, uint32_t gb) {
     WSB_CUDA_TRY(ctx_, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaError_t e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
     if (e == cudaSuccess) {
-        k_spmv_loop<<<ga, kThreads, kSpmvSmem, cs>>>(d_sys_, d_sp_);
-        k_update<<<gb, kThreads, 0, cs>>>(d_sys_, d_sp_);
-        k_pupdate<<<gb, kThreads, 0, cs>>>(d_sys_, d_sp_, h);
+        k_spmv_loop<<<ga, kPipeThreads, kSpmvSmem, cs>>>(d_sys_, d_sp_);
+        k_update<<<gb, kPipeThreads, kUpdSmem, cs>>>(d_sys_, d_sp_);
+        k_pupdate<<<gc, kThreads, 0, cs>>>(d_sys_, d_sp_, h);
         e = cudaStreamEndCapture(cs, &body);
     }
     cudaStreamDestroy(cs);
@@ -435,19 +454,20 @@ int Engine::capture_loop(uint32_t ga, uint32_t gb) {
     WSB_CUDA_TRY(ctx_, cudaGraphInstantiate(&exec_, graph_, 0));
     graph_grid_a_ = ga;
     graph_grid_b_ = gb;
+    graph_grid_c_ = gc;
     return WSB_OK;
 }
 
 int Engine::launch_init(const std::vector<uint32_t> &ids) {
-    WorkItem *ia = h_work_ + 2 * work_cap_, *ib = h_work_ + 3 * work_cap_;
+    WorkItem *ia = h_work_ + L_IA * work_cap_, *ib = h_work_ + L_IB * work_cap_;
     uint32_t na = 0, nb = 0;
     for (uint32_t s : ids) {
         const Slot &sl = *slots_[s];
         for (uint32_t t = 0; t < sl.A->n_stiles; ++t) ia[na++] = {s, t};
         for (uint32_t t = 0; t < sl.M->n_utiles; ++t) ib[nb++] = {s, t};
     }
-    if (na) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + 2 * work_cap_, ia, sizeof(WorkItem) * na, cudaMemcpyHostToDevice, stream_));
-    if (nb) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + 3 * work_cap_, ib, sizeof(WorkItem) * nb, cudaMemcpyHostToDevice, stream_));
+    if (na) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + L_IA * work_cap_, ia, sizeof(WorkItem) * na, cudaMemcpyHostToDevice, stream_));
+    if (nb) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + L_IB * work_cap_, ib, sizeof(WorkItem) * nb, cudaMemcpyHostToDevice, stream_));
     h_sp_->n_init_a = na;
     h_sp_->n_init_b = nb;
     return WSB_OK;
@@ -457,19 +477,15 @@ int Engine::launch_aux(const std::vector<uint32_t> &ids, int which) {
     if (ids.empty()) return WSB_OK;
     int rc = rebuild_work();  // make sure storage exists
     if (rc) return rc;
-    WorkItem *xb = h_work_ + 4 * work_cap_;
+    WorkItem *xb = h_work_ + L_X * work_cap_;
     uint32_t nb = 0;
     for (uint32_t s : ids) {
         const Slot &sl = *slots_[s];
         for (uint32_t t = 0; t < sl.M->n_utiles; ++t) xb[nb++] = {s, t};
     }
-    WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + 4 * work_cap_, xb, sizeof(WorkItem) * nb, cudaMemcpyHostToDevice, stream_));
-    h_sp_->aux_b = d_work_ + 4 * work_cap_;
+    WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + L_X * work_cap_, xb, sizeof(WorkItem) * nb, cudaMemcpyHostToDevice, stream_));
+    fill_list_ptrs();
     h_sp_->n_aux_b = nb;
-    h_sp_->work_a = d_work_;
-    h_sp_->work_b = d_work_ + work_cap_;
-    h_sp_->init_a = d_work_ + 2 * work_cap_;
-    h_sp_->init_b = d_work_ + 3 * work_cap_;
     WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_sp_, h_sp_, sizeof(StepParams), cudaMemcpyHostToDevice, stream_));
     const uint32_t g = std::min<uint32_t>(nb, (uint32_t)max_grid_b_);
     if (which == AUX_REFINE) k_refine<<<g, kThreads, 0, stream_>>>(d_sys_, d_sp_);
@@ -583,13 +599,11 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
     if (work_dirty_ && (rc = rebuild_work())) return rc;
     if ((rc = launch_init(init))) return rc;
     num_active_ = running + (uint32_t)init.size();
-    h_sp_->work_a = d_work_;
-    h_sp_->work_b = d_work_ + work_cap_;
-    h_sp_->init_a = d_work_ + 2 * work_cap_;
-    h_sp_->init_b = d_work_ + 3 * work_cap_;
-    h_sp_->aux_b = d_work_ + 4 * work_cap_;
+    fill_list_ptrs();
     h_sp_->n_work_a = n_work_a_;
     h_sp_->n_work_b = n_work_b_;
+    h_sp_->n_work_c = n_work_c_;
+    h_sp_->error = 0;
     // Bound the device loop by the largest remaining iteration budget: every
     // system stops by its own max_iter, so the loop ends even if one did not.
     uint64_t budget = 1;
@@ -608,17 +622,38 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
     if (!init.empty()) {
         const uint32_t ga = std::min<uint32_t>(h_sp_->n_init_a, (uint32_t)max_grid_a_);
         const uint32_t gb = std::min<uint32_t>(h_sp_->n_init_b, (uint32_t)max_grid_b_);
-        if (ga) k_spmv_init<<<ga, kThreads, kSpmvSmem, stream_>>>(d_sys_, d_sp_);
-        if (gb) k_init<<<gb, kThreads, 0, stream_>>>(d_sys_, d_sp_);
+        if (ga) k_spmv_init<<<ga, kPipeThreads, kSpmvSmem, stream_>>>(d_sys_, d_sp_);
+        if (gb) k_init<<<gb, kPipeThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
         WSB_CUDA_TRY(ctx_, cudaGetLastError());
         launches_ += (ga ? 1 : 0) + (gb ? 1 : 0);
     }
     if (num_active_ > 0 && n_work_a_ > 0) {
         const uint32_t ga = std::max<uint32_t>(1, std::min<uint32_t>(n_work_a_, (uint32_t)max_grid_a_));
         const uint32_t gb = std::max<uint32_t>(1, std::min<uint32_t>(n_work_b_, (uint32_t)max_grid_b_));
-        if (!exec_ || ga > graph_grid_a_ || gb > graph_grid_b_ || 2 * ga < graph_grid_a_ || 2 * gb < graph_grid_b_)
-            if ((rc = capture_loop(ga, gb))) return rc;
-        WSB_CUDA_TRY(ctx_, cudaGraphLaunch(exec_, stream_));
+        const uint32_t gc = std::max<uint32_t>(1, std::min<uint32_t>(n_work_c_, (uint32_t)max_grid_c_));
+        if (use_graph_) {
+            if (!exec_ || ga > graph_grid_a_ || gb > graph_grid_b_ || gc > graph_grid_c_ || 2 * ga < graph_grid_a_ ||
+                2 * gb < graph_grid_b_ || 2 * gc < graph_grid_c_)
+                if ((rc = capture_loop(ga, gb, gc))) return rc;
+            WSB_CUDA_TRY(ctx_, cudaGraphLaunch(exec_, stream_));
+        } else {
+            // Plain launches, polling the device state every 16 iterations.
+            uint32_t done_iters = 0;
+            while (done_iters < limit) {
+                const uint32_t burst = std::min<uint32_t>(16, limit - done_iters);
+                for (uint32_t i = 0; i < burst; ++i) {
+                    k_spmv_loop<<<ga, kPipeThreads, kSpmvSmem, stream_>>>(d_sys_, d_sp_);
+                    k_update<<<gb, kPipeThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
+                    k_pupdate<<<gc, kThreads, 0, stream_>>>(d_sys_, d_sp_, 0);
+                }
+                WSB_CUDA_TRY(ctx_, cudaGetLastError());
+                done_iters += burst;
+                WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(h_sp_rb_, d_sp_, sizeof(StepParams), cudaMemcpyDeviceToHost, stream_));
+                WSB_CUDA_TRY(ctx_, cudaStreamSynchronize(stream_));
+                if (h_sp_rb_->num_active == 0 || h_sp_rb_->error) break;
+            }
+            h_sp_->loop_count = done_iters;
+        }
     }
     if (timing) cudaEventRecord(ev1_, stream_);
     // 3) Read back states; retire or hand finished inner solves to refinement.
@@ -660,11 +695,81 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
     WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(h_sp_rb_, d_sp_, sizeof(StepParams), cudaMemcpyDeviceToHost, stream_));
     WSB_CUDA_TRY(ctx_, cudaStreamSynchronize(stream_));
     if (num_active_ > 0 && n_work_a_ > 0) launches_ += 1 + 3ull * h_sp_rb_->loop_count;
+    if (h_sp_rb_->error) {
+        // A bounded wait ran out inside a kernel: end every system in flight.
+        const uint32_t code = h_sp_rb_->error;
+        const int rc2 = (code & 7u) ? fail(ctx_, WSB_ERR_TIMEOUT, "a device wait ran out (kernel code %u)", code)
+                                    : fail(ctx_, WSB_ERR_CUDA, "a kernel met an invalid work item (code %u)", code);
+        for (uint32_t s2 = 0; s2 < slots_.size(); ++s2)
+            if (slots_[s2] && slots_[s2]->phase == Slot::RUNNING) finish_slot(s2, rc2);
+        h_sp_->error = 0;
+        WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_sp_, h_sp_, sizeof(StepParams), cudaMemcpyHostToDevice, stream_));
+        work_dirty_ = true;
+        return rc2;
+    }
     bool left = false;
     for (auto &sl : slots_)
         if (sl && (sl->phase == Slot::NEED_INIT || sl->phase == Slot::RUNNING || sl->phase == Slot::NEED_REFINE))
             left = true;
     *any_left = left;
+    return WSB_OK;
+}
+
+int Engine::profile_kernels(uint32_t s, uint32_t iters, double ms[3]) {
+    int rc;
+    Slot &sl = *slots_[s];
+    if (sl.A->n == 0 || iters == 0) return fail(ctx_, WSB_ERR_BAD_INPUT, "nothing to profile");
+    SysState &st = h_state_[s];
+    std::memset(&st, 0, sizeof st);
+    st.active = 1;
+    st.status = ST_RUNNING;
+    st.max_iter = iters + 1;  // tolerances 0: runs all iterations
+    if ((rc = push_state(s))) return rc;
+    sl.phase = Slot::RUNNING;
+    work_dirty_ = true;
+    if ((rc = rebuild_work())) return rc;
+    if ((rc = launch_init({s}))) return rc;
+    fill_list_ptrs();
+    h_sp_->n_work_a = n_work_a_;
+    h_sp_->n_work_b = n_work_b_;
+    h_sp_->n_work_c = n_work_c_;
+    h_sp_->error = 0;
+    h_sp_->num_active = 1;
+    h_sp_->loop_count = 0;
+    h_sp_->loop_limit = iters;
+    WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_sp_, h_sp_, sizeof(StepParams), cudaMemcpyHostToDevice, stream_));
+    const uint32_t ga = std::min<uint32_t>(n_work_a_, (uint32_t)max_grid_a_);
+    const uint32_t gb = std::min<uint32_t>(n_work_b_, (uint32_t)max_grid_b_);
+    const uint32_t gc = std::min<uint32_t>(n_work_c_, (uint32_t)max_grid_c_);
+    k_spmv_init<<<std::min<uint32_t>(h_sp_->n_init_a, (uint32_t)max_grid_a_), kPipeThreads, kSpmvSmem, stream_>>>(d_sys_, d_sp_);
+    k_init<<<std::min<uint32_t>(h_sp_->n_init_b, (uint32_t)max_grid_b_), kPipeThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
+    std::vector<cudaEvent_t> ev(4 * (size_t)iters);
+    for (auto &e : ev) WSB_CUDA_TRY(ctx_, cudaEventCreate(&e));
+    for (uint32_t i = 0; i < iters; ++i) {
+        cudaEventRecord(ev[4 * i + 0], stream_);
+        k_spmv_loop<<<ga, kPipeThreads, kSpmvSmem, stream_>>>(d_sys_, d_sp_);
+        cudaEventRecord(ev[4 * i + 1], stream_);
+        k_update<<<gb, kPipeThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
+        cudaEventRecord(ev[4 * i + 2], stream_);
+        k_pupdate<<<gc, kThreads, 0, stream_>>>(d_sys_, d_sp_, 0);
+        cudaEventRecord(ev[4 * i + 3], stream_);
+    }
+    WSB_CUDA_TRY(ctx_, cudaGetLastError());
+    WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(h_sp_rb_, d_sp_, sizeof(StepParams), cudaMemcpyDeviceToHost, stream_));
+    WSB_CUDA_TRY(ctx_, cudaStreamSynchronize(stream_));
+    if (h_sp_rb_->error) return fail(ctx_, (h_sp_rb_->error & 7u) ? WSB_ERR_TIMEOUT : WSB_ERR_CUDA,
+                                     "kernel error code %u during profiling", h_sp_rb_->error);
+    double acc[3] = {0, 0, 0};
+    for (uint32_t i = 0; i < iters; ++i)
+        for (int k = 0; k < 3; ++k) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ev[4 * i + k], ev[4 * i + k + 1]);
+            acc[k] += t;
+        }
+    for (auto &e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < 3; ++k) ms[k] = acc[k] / iters;
+    sl.phase = Slot::DONE;
+    work_dirty_ = true;
     return WSB_OK;
 }
 

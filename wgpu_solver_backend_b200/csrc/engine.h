@@ -82,6 +82,10 @@ class Engine {
     int fetch(uint32_t slot, float *x, bool device_ptr, bool always_x, SolveOutcome *out, double *hist,
               uint64_t hist_cap, uint64_t *hist_len, double *x64 = nullptr);
     int reset_slot(uint32_t slot, const SolveCfg &cfg);  // reuse for another solve
+    // Runs the init kernels and then `iters` loop iterations of one slot
+    // outside the graph with CUDA events around every launch; ms[0..2] get
+    // the mean duration of k_spmv_loop, k_update and k_pupdate.
+    int profile_kernels(uint32_t slot, uint32_t iters, double ms[3]);
     void remove(uint32_t slot);
     bool done(uint32_t slot) const;
     uint64_t slot_bytes(uint32_t slot) const;
@@ -96,7 +100,11 @@ class Engine {
 
   private:
     int ensure_capacity(uint32_t need);
-    int capture_loop(uint32_t grid_a, uint32_t grid_b);
+    int capture_loop(uint32_t grid_a, uint32_t grid_b, uint32_t grid_c);
+    void fill_list_ptrs();
+    static uint32_t chunks_of(uint32_t n) { return (n + kChunkRows - 1) / kChunkRows; }
+    // Work-list regions in d_work_ / h_work_ (work_cap_ items each).
+    enum { L_A = 0, L_B = 1, L_C = 2, L_IA = 3, L_IB = 4, L_X = 5, kLists = 6 };
     int push_desc(uint32_t slot);
     int push_state(uint32_t slot);
     int launch_init(const std::vector<uint32_t> &slots);
@@ -112,14 +120,15 @@ class Engine {
     SysDesc *d_sys_ = nullptr, *h_sys_ = nullptr;      // device array + pinned mirror
     SysState *d_state_ = nullptr, *h_state_ = nullptr;
     StepParams *d_sp_ = nullptr, *h_sp_ = nullptr, *h_sp_rb_ = nullptr;
-    WorkItem *d_work_ = nullptr, *h_work_ = nullptr;  // work_a | work_b | init_a | init_b | aux_b
+    WorkItem *d_work_ = nullptr, *h_work_ = nullptr;  // kLists regions
     size_t work_cap_ = 0;
-    uint32_t n_work_a_ = 0, n_work_b_ = 0;
+    uint32_t n_work_a_ = 0, n_work_b_ = 0, n_work_c_ = 0;
     bool work_dirty_ = true;
+    bool use_graph_ = true;   // WSB_LOOP=launch: plain launches + host polling
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;
-    uint32_t graph_grid_a_ = 0, graph_grid_b_ = 0;
-    int max_grid_a_ = 0, max_grid_b_ = 0;
+    uint32_t graph_grid_a_ = 0, graph_grid_b_ = 0, graph_grid_c_ = 0;
+    int max_grid_a_ = 0, max_grid_b_ = 0, max_grid_c_ = 0;
     uint32_t num_active_ = 0;
     double last_device_ms_ = 0.0;
     uint64_t launches_ = 0;

@@ -176,9 +176,9 @@ int validate_system(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, ui
     return WSB_OK;
 }
 
-// Greedy CSR row tiles: <= kTileRows rows and <= kCsrCap nonzeros, except a
-// single row longer than kCsrCap, which gets a tile of its own and is
-// streamed through shared memory in chunks by the kernel.
+// Greedy CSR row tiles: <= kTileRows rows and <= kCsrCap nonzeros (one TMA
+// stage), except a single row longer than kCsrCap, which gets a tile of its
+// own and is streamed through shared memory in chunks by the kernel.
 void build_spmv_tiles_csr(uint32_t n, const uint32_t *row_ptr, std::vector<SpmvTile> *out) {
     out->clear();
     uint32_t r0 = 0;
@@ -190,7 +190,7 @@ void build_spmv_tiles_csr(uint32_t n, const uint32_t *row_ptr, std::vector<SpmvT
             ++r1;
             if (tile_nnz > (uint64_t)kCsrCap) break;  // long single row
         }
-        out->push_back({r0, r1});
+        out->push_back({r0, r1, row_ptr[r0], row_ptr[r1]});
         r0 = r1;
     }
 }
@@ -209,35 +209,44 @@ void build_spmv_tiles_bsr(uint32_t nbrows, const uint32_t *brow_ptr, std::vector
             ++r1;
             if (blocks > (uint64_t)kBsrCapBlocks) break;
         }
-        out->push_back({r0, r1});
+        out->push_back({r0, r1, brow_ptr[r0], brow_ptr[r1]});
         r0 = r1;
     }
 }
 
-// Update tiles of <= kTileRows rows. A cut is allowed at a block start or at
-// a row whose position inside its block is >= 6 (the reference never touches
-// z there, block_jacobi.wgsl:79,124-126), so the solved rows of a block are
-// always inside one tile.
+// Update tiles of <= kTileRows rows holding <= kUpdBlocks block starts. A cut
+// is allowed at a block start or at a row whose position inside its block is
+// >= 6 (the reference never touches z there, block_jacobi.wgsl:79,124-126),
+// so the solved rows of a block are always inside one tile.
 void build_upd_tiles(uint32_t n, const uint32_t *bs, uint32_t nb, std::vector<UpdTile> *out) {
     out->clear();
     if (n == 0) return;
     std::vector<uint8_t> cut_ok(n + 1, 0);
+    std::vector<uint32_t> starts_before(n + 1, 0);  // block starts in [0, r)
     cut_ok[n] = 1;
     for (uint32_t b = 0; b < nb; ++b) {
         cut_ok[bs[b]] = 1;
         for (uint32_t r = bs[b] + 6; r < bs[b + 1]; ++r) cut_ok[r] = 1;
     }
-    uint32_t r0 = 0, blk = 0;
+    {
+        uint32_t b = 0;
+        for (uint32_t r = 0; r <= n; ++r) {
+            while (b < nb && bs[b] < r) ++b;
+            starts_before[r] = b;
+        }
+    }
+    uint32_t r0 = 0;
     while (r0 < n) {
         uint32_t r1 = std::min<uint32_t>(n, r0 + kTileRows);
-        while (!cut_ok[r1]) --r1;  // terminates: at worst the block start
+        while (r1 > r0 + 1 && (!cut_ok[r1] || starts_before[r1] - starts_before[r0] > (uint32_t)kUpdBlocks)) --r1;
+        // r0 + 1 is always a cut when the block at r0 has one row or r0 is a
+        // passive row; otherwise the loop stops at the next block start.
+        while (!cut_ok[r1]) ++r1;
         UpdTile t;
         t.row0 = r0;
         t.row1 = r1;
-        while (blk < nb && bs[blk] < r0) ++blk;
-        t.blk0 = blk;
-        while (blk < nb && bs[blk] < r1) ++blk;
-        t.blk1 = blk;
+        t.blk0 = starts_before[r0];
+        t.blk1 = starts_before[r1];
         out->push_back(t);
         r0 = r1;
     }

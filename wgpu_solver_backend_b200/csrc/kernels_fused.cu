@@ -1,27 +1,105 @@
 // Fused, batch-native PCG kernels for B200 (sm_100a).
 //
-// Memory-bound design notes (no dense contraction on this path, so no tensor
-// cores): every CTA works on row tiles taken from a device work list in a
-// grid-stride loop, so one captured CUDA graph serves any number of systems.
-// Matrix values/columns are streamed once per iteration with 128-bit
-// evict-first loads (ld.global.cs) into shared memory; the gathered vector is
-// read through the read-only path (ld.global.nc) and stays in the 126 MB L2.
-// Per-system reductions are deterministic: each tile writes one FP64 partial,
-// and the last CTA of a system (ticket counter) sums the partials in a fixed
-// order, so a system's arithmetic does not depend on how many other systems
-// share the launch.
+// Memory-bound design (no dense contraction on this path, so no tensor
+// cores). Every CTA is persistent over a device work list of row tiles (grid
+// = SMs x resident CTAs, grid-stride over the list), so one captured CUDA
+// graph serves any number of systems. The matrix and vector slices of a tile
+// are brought into shared memory with TMA bulk copies (cp.async.bulk +
+// mbarrier transaction counts) into a two-stage ring: while a CTA computes
+// tile k, tile k+1 is already streaming in, which keeps ~100 KB per SM in
+// flight. The gathered vector is read through the read-only path and stays
+// in the 126 MB L2. Per-system reductions are deterministic: every tile
+// writes one FP64 partial and the last CTA of a system (ticket counter) sums
+// them in a fixed order, so a system's arithmetic does not depend on what
+// else shares the launch.
 //
 // Arithmetic parity with the reference: SpMV rows are summed sequentially in
-// index order with separately rounded multiply and add (spmv.wgsl:58-61), the
-// vector updates are y + a*x without contraction (axpy*.wgsl), the block solve
-// is block_jacobi.wgsl:93-126 operation by operation, and p = p*beta + z
-// follows scale_from_scalar_results.wgsl then axpy.wgsl.
+// index order with separately rounded multiply and add (spmv.wgsl:58-61); the
+// vector updates are y + a*x without contraction (axpy*.wgsl); the block
+// solve is block_jacobi.wgsl:93-126 operation by operation; p = p*beta + z is
+// scale_from_scalar_results.wgsl then axpy.wgsl.
+//
+// Every mbarrier wait is bounded (about 2 s of clock); a wait that runs out
+// records an error code in StepParams::error, waits (bounded) for the CTA's
+// own copies in flight and returns, and the host reports WSB_ERR_TIMEOUT.
 #include "kernels_fused.cuh"
 
 namespace wsb {
 
 namespace {
 
+// ---------------------------------------------------------------------------
+// TMA bulk copies and mbarriers (inline PTX).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// Orders this thread's generic-proxy shared-memory accesses before later
+// async-proxy (TMA) writes to the same buffers.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// 1-D bulk copy global -> shared; 16-byte aligned addresses, size % 16 == 0.
+__device__ __forceinline__ void tma_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\tmbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\tselp.u32 %0, 1, 0, P;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+constexpr long long kWaitCycles = 4000000000ll;  // about 2 s at 1.9 GHz
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > kWaitCycles) return false;
+    return true;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// The pipelined kernels run kThreads consumer threads (warps 0-7) and one
+// producer warp (kPipeThreads in all); consumers synchronise among themselves
+// on named barrier 1 so the producer never has to join. Kernels without a
+// producer warp launch exactly kThreads threads and use the same barrier.
+
+__device__ __forceinline__ void csync() { asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory"); }
+
+// Consumer thread 0 waits (bounded) and shares the outcome; then every
+// consumer observes the completed phase itself (immediate), which makes the
+// TMA data and the producer's descriptor visible to it.
+__device__ __forceinline__ bool consumer_wait(uint64_t *bar, uint32_t parity, int *s_ok) {
+    if (threadIdx.x == 0) *s_ok = mbar_wait(bar, parity) ? 1 : 0;
+    csync();
+    if (!*s_ok) return false;
+    mbar_wait(bar, parity);
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Reductions
+// ---------------------------------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -33,13 +111,13 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
     v = warp_sum(v);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (lane == 0) red[w] = v;
-    __syncthreads();
+    csync();
     double s = 0.0;
     if (w == 0) {
         s = lane < (kThreads >> 5) ? red[lane] : 0.0;
         s = warp_sum(s);
     }
-    __syncthreads();
+    csync();
     return s;
 }
 
@@ -51,7 +129,7 @@ __device__ __forceinline__ double2 block_sum2(double a, double b, double *red) {
         red[w] = a;
         red[32 + w] = b;
     }
-    __syncthreads();
+    csync();
     double sa = 0.0, sb = 0.0;
     if (w == 0) {
         sa = lane < (kThreads >> 5) ? red[lane] : 0.0;
@@ -59,459 +137,713 @@ __device__ __forceinline__ double2 block_sum2(double a, double b, double *red) {
         sa = warp_sum(sa);
         sb = warp_sum(sb);
     }
-    __syncthreads();
+    csync();
     return make_double2(sa, sb);
 }
 
-// Ticket on a per-system counter after thread 0 published this CTA's partial.
-// Returns true in every thread of the CTA that took the last ticket.
-__device__ __forceinline__ bool take_ticket(uint32_t *counter, uint32_t total, int *s_last) {
+// Ticket on a per-system counter: this CTA adds the number of tiles whose
+// partials it has published (thread 0 wrote them); true in every thread of
+// the CTA whose tickets complete the system's total.
+__device__ __forceinline__ bool take_ticket(uint32_t *counter, uint32_t cnt, uint32_t total, int *s_last) {
     if (threadIdx.x == 0) {
         __threadfence();
-        const uint32_t t = atomicAdd(counter, 1u);
-        *s_last = (t + 1 == total);
+        const uint32_t t = atomicAdd(counter, cnt);
+        *s_last = (t + cnt == total);
     }
-    __syncthreads();
+    csync();
     const bool last = *s_last != 0;
     if (last) __threadfence();
     return last;
 }
 
-// y(row0 + t) for the t < nrows rows of one CSR tile. The tile's nonzeros
-// [row_ptr[row0], row_ptr[row0+nrows]) are streamed in chunks of kCsrCap:
-// 16-byte aligned float4/uint4 loads, products val*x[col] stored in shared
-// memory, then one thread per row adds its products in index order.
-__device__ __forceinline__ float csr_rows(const SysDesc &S, uint32_t row0, uint32_t nrows,
-                                          const float *__restrict__ xin, float *prod, uint32_t *rp) {
-    const uint32_t tid = threadIdx.x;
-    const uint32_t *__restrict__ row_ptr = S.row_ptr;
-    const float *__restrict__ val = S.val;
-    const uint32_t *__restrict__ col = S.col;
-    for (uint32_t i = tid; i <= nrows; i += kThreads) rp[i] = __ldg(row_ptr + row0 + i);
-    __syncthreads();
-    const uint32_t k0 = rp[0], k1 = rp[nrows];
-    uint32_t ms = 0, me = 0;
-    if (tid < nrows) {
-        ms = rp[tid];
-        me = rp[tid + 1];
-    }
-    float acc = 0.0f;
-    for (uint32_t c0 = k0; c0 < k1; c0 += kCsrCap) {
-        const uint32_t c1 = min(k1, c0 + (uint32_t)kCsrCap);
-        const uint32_t a0 = c0 & ~3u;
-        uint32_t q = a0 + 4u * tid;
-        for (; q + 4u * kThreads < c1; q += 8u * kThreads) {
-            const float4 v0 = __ldcs(reinterpret_cast<const float4 *>(val + q));
-            const uint4 i0 = __ldcs(reinterpret_cast<const uint4 *>(col + q));
-            const float4 v1 = __ldcs(reinterpret_cast<const float4 *>(val + q + 4u * kThreads));
-            const uint4 i1 = __ldcs(reinterpret_cast<const uint4 *>(col + q + 4u * kThreads));
-            const float x00 = __ldg(xin + i0.x), x01 = __ldg(xin + i0.y), x02 = __ldg(xin + i0.z),
-                        x03 = __ldg(xin + i0.w);
-            const float x10 = __ldg(xin + i1.x), x11 = __ldg(xin + i1.y), x12 = __ldg(xin + i1.z),
-                        x13 = __ldg(xin + i1.w);
-            *reinterpret_cast<float4 *>(prod + (q - a0)) =
-                make_float4(__fmul_rn(v0.x, x00), __fmul_rn(v0.y, x01), __fmul_rn(v0.z, x02), __fmul_rn(v0.w, x03));
-            *reinterpret_cast<float4 *>(prod + (q + 4u * kThreads - a0)) =
-                make_float4(__fmul_rn(v1.x, x10), __fmul_rn(v1.y, x11), __fmul_rn(v1.z, x12), __fmul_rn(v1.w, x13));
-        }
-        if (q < c1) {
-            const float4 v0 = __ldcs(reinterpret_cast<const float4 *>(val + q));
-            const uint4 i0 = __ldcs(reinterpret_cast<const uint4 *>(col + q));
-            *reinterpret_cast<float4 *>(prod + (q - a0)) =
-                make_float4(__fmul_rn(v0.x, __ldg(xin + i0.x)), __fmul_rn(v0.y, __ldg(xin + i0.y)),
-                            __fmul_rn(v0.z, __ldg(xin + i0.z)), __fmul_rn(v0.w, __ldg(xin + i0.w)));
-        }
-        __syncthreads();
-        const uint32_t s = max(ms, c0), e = min(me, c1);
-        for (uint32_t j = s; j < e; ++j) acc = __fadd_rn(acc, prod[j - a0]);
-        __syncthreads();
-    }
-    return acc;
-}
+// ---------------------------------------------------------------------------
+// SpMV tiles
+// ---------------------------------------------------------------------------
+enum SpmvMode { M_LOOP = 0, M_INIT = 1, M_PLAIN = 2 };
 
-// y for the 6*nbrows rows of one BSR6 tile: 144-byte blocks staged with
-// float4 loads; thread t owns row (t/6, t%6) and walks its block row's blocks
-// in column order, six products each, added in index order. For a matrix that
-// stores complete 6x6 blocks with sorted columns this is exactly the CSR row
-// order, so both layouts round identically.
-__device__ __forceinline__ float bsr_rows(const SysDesc &S, uint32_t brow0, uint32_t nbrows,
-                                          const float *__restrict__ xin, float *sval, uint32_t *rp) {
-    const uint32_t tid = threadIdx.x;
-    uint32_t *scol = reinterpret_cast<uint32_t *>(sval + kBsrCapBlocks * 36);
-    for (uint32_t i = tid; i <= nbrows; i += kThreads) rp[i] = __ldg(S.brow_ptr + brow0 + i);
-    __syncthreads();
-    const uint32_t k0 = rp[0], k1 = rp[nbrows];
-    const uint32_t br = tid / 6u, a = tid - 6u * br;
-    uint32_t ms = 0, me = 0;
-    if (tid < 6u * nbrows) {
-        ms = rp[br];
-        me = rp[br + 1];
-    }
-    float acc = 0.0f;
-    for (uint32_t c0 = k0; c0 < k1; c0 += kBsrCapBlocks) {
-        const uint32_t c1 = min(k1, c0 + (uint32_t)kBsrCapBlocks);
-        const uint32_t nblk = c1 - c0;
-        const float4 *__restrict__ src = reinterpret_cast<const float4 *>(S.bval) + (size_t)c0 * 9u;
-        float4 *dst = reinterpret_cast<float4 *>(sval);
-        for (uint32_t q = tid; q < nblk * 9u; q += kThreads) dst[q] = __ldcs(src + q);
-        for (uint32_t q = tid; q < nblk; q += kThreads) scol[q] = __ldcs(S.bcol + c0 + q);
-        __syncthreads();
-        const uint32_t s = max(ms, c0), e = min(me, c1);
-        for (uint32_t blk = s; blk < e; ++blk) {
-            const float *B = sval + (blk - c0) * 36u + a * 6u;
-            const float2 *xx = reinterpret_cast<const float2 *>(xin + 6u * (size_t)scol[blk - c0]);
-            const float2 x01 = __ldg(xx), x23 = __ldg(xx + 1), x45 = __ldg(xx + 2);
-            acc = __fadd_rn(acc, __fmul_rn(B[0], x01.x));
-            acc = __fadd_rn(acc, __fmul_rn(B[1], x01.y));
-            acc = __fadd_rn(acc, __fmul_rn(B[2], x23.x));
-            acc = __fadd_rn(acc, __fmul_rn(B[3], x23.y));
-            acc = __fadd_rn(acc, __fmul_rn(B[4], x45.x));
-            acc = __fadd_rn(acc, __fmul_rn(B[5], x45.y));
-        }
-        __syncthreads();
-    }
-    return acc;
-}
+// Shared-memory stage (floats). CSR: values [0, kCsrCap+8), columns
+// [kCsrCap+8, 2(kCsrCap+8)), row pointers at kRpOff. BSR6: block values
+// [0, 36 kBsrCapBlocks), block columns at kBcolOff, row pointers at kRpOff.
+constexpr int kValCap = kCsrCap + 8;
+constexpr int kColOff = kValCap;
+constexpr int kBcolOff = kBsrCapBlocks * 36;
+constexpr int kRpOff = 2 * kValCap;
+constexpr int kXgOff = kBcolOff + kBsrCapBlocks + 8;  // BSR6: gathered x, 6 per block
+static_assert(kXgOff + 6 * kBsrCapBlocks <= kRpOff, "BSR stage fits");
+static_assert((kColOff * 4) % 16 == 0 && (kBcolOff * 4) % 16 == 0 && (kRpOff * 4) % 16 == 0, "TMA alignment");
+static_assert(kSpmvStageFloats >= kRpOff + kTileRows + 8, "stage size");
 
-// Rows [row0, row0+nrows) of A*xin for one SpMV tile of either layout.
-struct TileRows {
-    float acc;
-    uint32_t row0, nrows;
+struct SpmvDesc {
+    uint32_t valid, sys, tile, layout;
+    uint32_t r0, nr;  // tile rows in layout units (rows, or block rows)
+    uint32_t k0, k1;  // nonzero (block) range
+    uint32_t ka, ra;  // 4-aligned starts of the staged column / row-pointer ranges
+    uint32_t lng;     // a single row longer than a stage: synchronous path
+    uint32_t pad;
 };
 
-__device__ __forceinline__ TileRows tile_spmv(const SysDesc &S, const SpmvTile &T, const float *__restrict__ xin,
-                                              float *buf, uint32_t *rp) {
-    TileRows out;
-    if (S.layout == LAYOUT_BSR6) {
-        out.row0 = 6u * T.row0;
-        out.nrows = 6u * (T.row1 - T.row0);
-        out.acc = bsr_rows(S, T.row0, T.row1 - T.row0, xin, buf, rp);
+// Resolves the next tile of this CTA (thread 0). *w is the CTA's cursor.
+template <int kMode>
+__device__ __forceinline__ bool resolve_spmv(const SysDesc *__restrict__ sys, const StepParams *sp, uint32_t *w,
+                                             SpmvDesc *d) {
+    if (kMode == M_PLAIN) {
+        const SysDesc &S = sys[0];
+        if (*w >= S.n_stiles) return false;
+        d->sys = 0;
+        d->tile = *w;
+        *w += gridDim.x;
     } else {
-        out.row0 = T.row0;
-        out.nrows = T.row1 - T.row0;
-        out.acc = csr_rows(S, T.row0, T.row1 - T.row0, xin, buf, rp);
+        const uint32_t nw = kMode == M_INIT ? sp->n_init_a : sp->n_work_a;
+        const WorkItem *work = kMode == M_INIT ? sp->init_a : sp->work_a;
+        for (;;) {
+            if (*w >= nw) return false;
+            const WorkItem it = work[*w];
+            *w += gridDim.x;
+            if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_stiles) {
+                atomicOr(const_cast<uint32_t *>(&sp->error), 8u);  // invalid work item: skipped
+                continue;
+            }
+            if (kMode == M_LOOP && !sys[it.sys].st->active) continue;
+            d->sys = it.sys;
+            d->tile = it.tile;
+            break;
+        }
     }
-    return out;
+    const SysDesc &S = sys[d->sys];
+    const SpmvTile T = S.stiles[d->tile];
+    d->layout = S.layout;
+    d->r0 = T.row0;
+    d->nr = T.row1 - T.row0;
+    d->k0 = T.k0;
+    d->k1 = T.k1;
+    d->ka = T.k0 & ~3u;
+    d->ra = T.row0 & ~3u;
+    d->lng = (S.layout == LAYOUT_BSR6) ? (T.k1 - T.k0 > (uint32_t)kBsrCapBlocks) : (T.k1 - T.k0 > (uint32_t)kCsrCap);
+    return true;
 }
 
-// z = U^-1 L^-1 r for the blocks that start inside the tile (block_jacobi.wgsl:
-// forward solve with unit L, lines 93-101; backward solve dividing by U(i,i),
-// lines 103-122; rows i < m = min(6, len) only, lines 79 and 124-126). LU
-// factors (144 B per block) are staged through shared memory with coalesced
-// float4 loads, kLuStage blocks per pass; one thread solves one block in
-// registers. sr: the tile's r; outputs sz and sflag (1 where z was solved).
-__device__ __forceinline__ void bj_tile(const SysDesc &S, const UpdTile &T, const float *sr, float *sz,
-                                        uint32_t *sflag, float *slu) {
-    const uint32_t nblk = T.blk1 - T.blk0;
-    for (uint32_t pb = 0; pb < nblk; pb += kLuStage) {
-        const uint32_t nbp = min(nblk - pb, (uint32_t)kLuStage);
-        const float4 *__restrict__ src = reinterpret_cast<const float4 *>(S.lu) + (size_t)(T.blk0 + pb) * 9u;
-        float4 *dst = reinterpret_cast<float4 *>(slu);
-        for (uint32_t q = threadIdx.x; q < nbp * 9u; q += kThreads) dst[q] = __ldcs(src + q);
-        __syncthreads();
-        if (threadIdx.x < nbp) {
-            const uint32_t blk = T.blk0 + pb + threadIdx.x;
-            const uint32_t off = __ldg(S.bstart + blk), nxt = __ldg(S.bstart + blk + 1);
-            const uint32_t m = min(nxt - off, 6u);
-            const uint32_t lo = off - T.row0;
-            const float *L = slu + threadIdx.x * 36u;
-            float y[6], xs[6];
-#pragma unroll
-            for (int i = 0; i < 6; ++i) {
-                y[i] = 0.0f;
-                xs[i] = 0.0f;
-            }
-#pragma unroll
-            for (int i = 0; i < 6; ++i) {
-                if ((uint32_t)i < m) {
-                    float s = sr[lo + i];
-#pragma unroll
-                    for (int j = 0; j < i; ++j) s = __fsub_rn(s, __fmul_rn(L[i * 6 + j], y[j]));
-                    y[i] = s;
-                }
-            }
-#pragma unroll
-            for (int i = 5; i >= 0; --i) {
-                if ((uint32_t)i < m) {
-                    float s = y[i];
-#pragma unroll
-                    for (int j = i + 1; j < 6; ++j)
-                        if ((uint32_t)j < m) s = __fsub_rn(s, __fmul_rn(L[i * 6 + j], xs[j]));
-                    xs[i] = __fdiv_rn(s, L[i * 6 + i]);
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < 6; ++i)
-                if ((uint32_t)i < m) {
-                    sz[lo + i] = xs[i];
-                    sflag[lo + i] = 1u;
-                }
-        }
-        __syncthreads();
+// Issues the bulk copies of a resolved tile into a stage (thread 0).
+__device__ __forceinline__ void issue_spmv(const SysDesc *__restrict__ sys, const SpmvDesc &d, float *stage,
+                                           uint64_t *bar) {
+    if (d.lng) {
+        mbar_expect_tx(bar, 0);
+        return;
     }
+    const SysDesc &S = sys[d.sys];
+    const uint32_t rc = ((d.r0 + d.nr + 1 - d.ra) + 3) & ~3u;
+    const uint32_t cc = ((d.k1 - d.ka) + 3) & ~3u;
+    uint32_t *rp = reinterpret_cast<uint32_t *>(stage + kRpOff);
+    if (d.layout == LAYOUT_BSR6) {
+        const uint32_t vb = (d.k1 - d.k0) * 144u;
+        mbar_expect_tx(bar, vb + 4u * cc + 4u * rc);
+        if (vb) tma_load(stage, S.bval + (size_t)d.k0 * 36u, vb, bar);
+        if (cc) tma_load(stage + kBcolOff, S.bcol + d.ka, 4u * cc, bar);
+        tma_load(rp, S.brow_ptr + d.ra, 4u * rc, bar);
+    } else {
+        mbar_expect_tx(bar, 8u * cc + 4u * rc);
+        if (cc) {
+            tma_load(stage, S.val + d.ka, 4u * cc, bar);
+            tma_load(stage + kColOff, S.col + d.ka, 4u * cc, bar);
+        }
+        tma_load(rp, S.row_ptr + d.ra, 4u * rc, bar);
+    }
+}
+
+// CSR tile from a filled stage: products val*x[col] in place (all threads,
+// strided over the nonzeros), then one thread per row adds its products in
+// index order.
+__device__ __forceinline__ float csr_stage(const SpmvDesc &d, const float *__restrict__ xin, float *stage) {
+    float *val = stage;
+    const uint32_t *col = reinterpret_cast<const uint32_t *>(stage + kColOff);
+    const uint32_t *rp = reinterpret_cast<const uint32_t *>(stage + kRpOff);
+    const uint32_t j0 = d.k0 - d.ka, j1 = d.k1 - d.ka;
+    uint32_t j = j0 + threadIdx.x;
+    for (; j + 3 * kThreads < j1; j += 4 * kThreads) {
+        const uint32_t c0 = col[j], c1 = col[j + kThreads], c2 = col[j + 2 * kThreads], c3 = col[j + 3 * kThreads];
+        const float x0 = __ldg(xin + c0), x1 = __ldg(xin + c1), x2 = __ldg(xin + c2), x3 = __ldg(xin + c3);
+        val[j] = __fmul_rn(val[j], x0);
+        val[j + kThreads] = __fmul_rn(val[j + kThreads], x1);
+        val[j + 2 * kThreads] = __fmul_rn(val[j + 2 * kThreads], x2);
+        val[j + 3 * kThreads] = __fmul_rn(val[j + 3 * kThreads], x3);
+    }
+    for (; j < j1; j += kThreads) val[j] = __fmul_rn(val[j], __ldg(xin + col[j]));
+    csync();
+    float acc = 0.0f;
+    if (threadIdx.x < d.nr) {
+        const uint32_t o = d.r0 - d.ra + threadIdx.x;
+        const uint32_t s = rp[o] - d.ka, e = rp[o + 1] - d.ka;
+        for (uint32_t q = s; q < e; ++q) acc = __fadd_rn(acc, val[q]);
+    }
+    return acc;
+}
+
+// BSR6 tile from a filled stage. Phase A (all threads): the 6 x values of
+// every block column are gathered into shared memory, with independent loads.
+// Phase B: thread t owns row (t/6, t%6) and walks its block row's blocks in
+// column order, six products each from shared memory, added in index order
+// (for complete 6x6 blocks with sorted columns this is the CSR order).
+__device__ __forceinline__ float bsr_stage(const SpmvDesc &d, const float *__restrict__ xin, float *stage) {
+    const uint32_t *bcol = reinterpret_cast<const uint32_t *>(stage + kBcolOff);
+    const uint32_t *rp = reinterpret_cast<const uint32_t *>(stage + kRpOff);
+    float *xg = stage + kXgOff;
+    const uint32_t nb = d.k1 - d.k0, cofs = d.k0 - d.ka;
+    const uint32_t ne = 6u * nb;
+    uint32_t e = threadIdx.x;
+    for (; e + 3 * kThreads < ne; e += 4 * kThreads) {
+        const uint32_t e1 = e + kThreads, e2 = e + 2 * kThreads, e3 = e + 3 * kThreads;
+        const float v0 = __ldg(xin + 6u * (size_t)bcol[e / 6u + cofs] + e % 6u);
+        const float v1 = __ldg(xin + 6u * (size_t)bcol[e1 / 6u + cofs] + e1 % 6u);
+        const float v2 = __ldg(xin + 6u * (size_t)bcol[e2 / 6u + cofs] + e2 % 6u);
+        const float v3 = __ldg(xin + 6u * (size_t)bcol[e3 / 6u + cofs] + e3 % 6u);
+        xg[e] = v0;
+        xg[e1] = v1;
+        xg[e2] = v2;
+        xg[e3] = v3;
+    }
+    for (; e < ne; e += kThreads) xg[e] = __ldg(xin + 6u * (size_t)bcol[e / 6u + cofs] + e % 6u);
+    csync();
+    float acc = 0.0f;
+    const uint32_t t = threadIdx.x;
+    if (t < 6u * d.nr) {
+        const uint32_t br = t / 6u, a = t - 6u * br;
+        const uint32_t o = d.r0 - d.ra + br;
+        const uint32_t s0 = rp[o] - d.k0, s1 = rp[o + 1] - d.k0;
+        for (uint32_t blk = s0; blk < s1; ++blk) {
+            const float *B = stage + blk * 36u + a * 6u;
+            const float *X = xg + blk * 6u;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) acc = __fadd_rn(acc, __fmul_rn(B[j], X[j]));
+        }
+    }
+    return acc;
+}
+
+// A tile whose single row (or block row) exceeds a stage: staged in chunks
+// with plain loads, using the stage as scratch (no copy is in flight into it).
+__device__ __forceinline__ float long_tile(const SysDesc &S, const SpmvDesc &d, const float *__restrict__ xin, float *stage) {
+    const uint32_t t = threadIdx.x;
+    float acc = 0.0f;
+    if (d.layout == LAYOUT_BSR6) {
+        // One block row of 6 rows, blocks [k0, k1) in chunks of kBsrCapBlocks.
+        uint32_t *bcol = reinterpret_cast<uint32_t *>(stage + kBcolOff);
+        for (uint32_t c0 = d.k0; c0 < d.k1; c0 += kBsrCapBlocks) {
+            const uint32_t nb = min(d.k1 - c0, (uint32_t)kBsrCapBlocks);
+            const float4 *src = reinterpret_cast<const float4 *>(S.bval) + (size_t)c0 * 9u;
+            float4 *dst = reinterpret_cast<float4 *>(stage);
+            for (uint32_t q = t; q < nb * 9u; q += kThreads) dst[q] = __ldcs(src + q);
+            for (uint32_t q = t; q < nb; q += kThreads) bcol[q] = __ldcs(S.bcol + c0 + q);
+            csync();
+            if (t < 6u) {
+                for (uint32_t blk = 0; blk < nb; ++blk) {
+                    const float *B = stage + blk * 36u + t * 6u;
+                    const float *xx = xin + 6u * (size_t)bcol[blk];
+#pragma unroll
+                    for (int jj = 0; jj < 6; ++jj) acc = __fadd_rn(acc, __fmul_rn(B[jj], __ldg(xx + jj)));
+                }
+            }
+            csync();
+        }
+        return acc;
+    }
+    // One CSR row, nonzeros [k0, k1) in chunks of 2 kCsrCap products.
+    constexpr uint32_t kChunk = 2 * kCsrCap;
+    for (uint32_t c0 = d.k0; c0 < d.k1; c0 += kChunk) {
+        const uint32_t c1 = min(d.k1, c0 + kChunk);
+        for (uint32_t q = c0 + t; q < c1; q += kThreads)
+            stage[q - c0] = __fmul_rn(__ldcs(S.val + q), __ldg(xin + __ldcs(S.col + q)));
+        csync();
+        if (t == 0)
+            for (uint32_t q = c0; q < c1; ++q) acc = __fadd_rn(acc, stage[q - c0]);
+        csync();
+    }
+    return acc;
+}
+
+// The last CTA of a system's SpMV tiles: p.Ap from the per-tile partials in
+// tile order, alpha = rz_old / pAp (0 when pAp == 0, as
+// pcg_update_scalars.wgsl:59-62).
+__device__ __forceinline__ void flush_spmv(const SysDesc *__restrict__ sys, uint32_t s, uint32_t cnt, double *red,
+                                           int *s_last) {
+    if (cnt == 0) return;
+    const SysDesc &S = sys[s];
+    SysState *st = S.st;
+    if (!take_ticket(&st->cnt_a, cnt, S.n_stiles, s_last)) return;
+    double v = 0.0;
+    for (uint32_t i = threadIdx.x; i < S.n_stiles; i += kThreads) v += __ldcg(S.part_a + i);
+    const double pap = block_sum(v, red);
+    if (threadIdx.x == 0) {
+        const double alpha = pap != 0.0 ? st->rz_old / pap : 0.0;
+        st->pap = pap;
+        st->alpha = alpha;
+        st->alpha_f = (float)alpha;
+        st->cnt_a = 0;
+    }
+}
+
+// The SpMV pipeline shared by the loop, init and plain kernels. Thread
+// kThreads (lane 0 of the producer warp) resolves tiles and issues their TMA
+// copies into a two-stage ring (full barrier: copy bytes; empty barrier: one
+// arrival per consumer); the consumers compute tile after tile.
+template <int kMode>
+__device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, StepParams *sp,
+                                              const float *__restrict__ xplain, float *__restrict__ yplain,
+                                              float *smem) {
+    __shared__ __align__(8) uint64_t full[2], empty[2];
+    __shared__ SpmvDesc desc[2];
+    __shared__ double red[64];
+    __shared__ int s_last, s_ok;
+    const uint32_t tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        mbar_init(&empty[0], kThreads);
+        mbar_init(&empty[1], kThreads);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid >= kThreads) {
+        if (tid != kThreads) return;
+        uint32_t w = blockIdx.x;
+        for (uint32_t k = 0;; ++k) {
+            const uint32_t s = k & 1u;
+            if (k >= 2 && !mbar_wait(&empty[s], ((k >> 1) - 1) & 1u)) {
+                atomicOr(&sp->error, 16u);
+                return;
+            }
+            SpmvDesc d;
+            d.valid = resolve_spmv<kMode>(sys, sp, &w, &d) ? 1u : 0u;
+            desc[s] = d;
+            if (d.valid) {
+                issue_spmv(sys, d, smem + s * kSpmvStageFloats, &full[s]);
+            } else {
+                mbar_expect_tx(&full[s], 0);
+                return;
+            }
+        }
+    }
+    uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles published since the last ticket
+    for (uint32_t k = 0;; ++k) {
+        const uint32_t s = k & 1u;
+        if (!consumer_wait(&full[s], (k >> 1) & 1u, &s_ok)) {
+            if (tid == 0) {
+                atomicOr(&sp->error, 1u);
+                mbar_wait(&full[s ^ 1u], ((k + 1) >> 1) & 1u);  // bounded drain of the other stage
+            }
+            return;
+        }
+        const SpmvDesc d = desc[s];
+        if (!d.valid) break;
+        float *stage = smem + s * kSpmvStageFloats;
+        const SysDesc &S = sys[d.sys];
+        const float *__restrict__ xin = kMode == M_PLAIN ? xplain : kMode == M_INIT ? S.x : S.p;
+        float acc;
+        if (d.lng) acc = long_tile(S, d, xin, stage);
+        else if (d.layout == LAYOUT_BSR6) acc = bsr_stage(d, xin, stage);
+        else acc = csr_stage(d, xin, stage);
+        const uint32_t row0 = d.layout == LAYOUT_BSR6 ? 6u * d.r0 : d.r0;
+        const uint32_t nrows = d.layout == LAYOUT_BSR6 ? 6u * d.nr : d.nr;
+        // Everyone is done reading the stage: hand it back to the producer.
+        fence_proxy_async();
+        mbar_arrive(&empty[s]);
+        if (kMode == M_PLAIN) {
+            if (tid < nrows) yplain[row0 + tid] = acc;
+        } else {
+            double part = 0.0;
+            if (tid < nrows) {
+                const uint32_t i = row0 + tid;
+                S.ap[i] = acc;
+                if (kMode == M_LOOP) part = (double)__ldg(xin + i) * (double)acc;
+            }
+            if (kMode == M_LOOP) {
+                const double tot = block_sum(part, red);
+                if (d.sys != run_sys) {
+                    flush_spmv(sys, run_sys, run_cnt, red, &s_last);
+                    run_sys = d.sys;
+                    run_cnt = 0;
+                }
+                if (tid == 0) S.part_a[d.tile] = tot;
+                ++run_cnt;
+            }
+        }
+    }
+    if (kMode == M_LOOP && run_sys != 0xffffffffu) flush_spmv(sys, run_sys, run_cnt, red, &s_last);
+}
+
+// ---------------------------------------------------------------------------
+// Update tiles (x, r, z and the block-Jacobi solve)
+// ---------------------------------------------------------------------------
+constexpr int kVecCap = kTileRows + 8;                    // floats per staged vector slice
+constexpr int kLuOff = 4 * kVecCap;                       // LU blocks
+constexpr int kBsOff = kLuOff + kUpdBlocks * 36;          // block starts slice
+static_assert((kLuOff * 4) % 16 == 0 && (kBsOff * 4) % 16 == 0 && (kVecCap * 4) % 16 == 0, "TMA alignment");
+static_assert(kUpdStageFloats >= kBsOff + kUpdBlocks + 8, "stage size");
+
+struct UpdDesc {
+    uint32_t valid, sys, tile;
+    uint32_t row0, rows, blk0, nblk;
+    uint32_t ra, ba;  // 4-aligned starts of the staged row / block-start ranges
+    uint32_t pad[3];
+};
+
+template <bool kInit>
+__device__ __forceinline__ bool resolve_upd(const SysDesc *__restrict__ sys, const StepParams *sp, uint32_t *w,
+                                            UpdDesc *d) {
+    const uint32_t nw = kInit ? sp->n_init_b : sp->n_work_b;
+    const WorkItem *work = kInit ? sp->init_b : sp->work_b;
+    for (;;) {
+        if (*w >= nw) return false;
+        const WorkItem it = work[*w];
+        *w += gridDim.x;
+        if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_utiles) {
+            atomicOr(const_cast<uint32_t *>(&sp->error), 8u);  // invalid work item: skipped
+            continue;
+        }
+        if (!kInit && !sys[it.sys].st->active) continue;
+        const UpdTile T = sys[it.sys].utiles[it.tile];
+        d->sys = it.sys;
+        d->tile = it.tile;
+        d->row0 = T.row0;
+        d->rows = T.row1 - T.row0;
+        d->blk0 = T.blk0;
+        d->nblk = T.blk1 - T.blk0;
+        d->ra = T.row0 & ~3u;
+        d->ba = T.blk0 & ~3u;
+        return true;
+    }
+}
+
+// Stage slots: 0 = x (init: b), 1 = p, 2 = r, 3 = Ap; then LU and block starts.
+template <bool kInit>
+__device__ __forceinline__ void issue_upd(const SysDesc *__restrict__ sys, const UpdDesc &d, float *stage,
+                                          uint64_t *bar) {
+    const SysDesc &S = sys[d.sys];
+    const uint32_t vc = ((d.row0 + d.rows - d.ra) + 3) & ~3u;
+    const uint32_t bc = ((d.blk0 + d.nblk + 1 - d.ba) + 3) & ~3u;
+    const uint32_t lub = d.nblk * 144u;
+    const uint32_t nvec = kInit ? 2u : 4u;
+    mbar_expect_tx(bar, nvec * 4u * vc + lub + 4u * bc);
+    if (kInit) {
+        tma_load(stage, S.b + d.ra, 4u * vc, bar);
+        tma_load(stage + 3 * kVecCap, S.ap + d.ra, 4u * vc, bar);
+    } else {
+        tma_load(stage, S.x + d.ra, 4u * vc, bar);
+        tma_load(stage + kVecCap, S.p + d.ra, 4u * vc, bar);
+        tma_load(stage + 2 * kVecCap, S.r + d.ra, 4u * vc, bar);
+        tma_load(stage + 3 * kVecCap, S.ap + d.ra, 4u * vc, bar);
+    }
+    if (lub) tma_load(stage + kLuOff, S.lu + (size_t)d.blk0 * 36u, lub, bar);
+    tma_load(stage + kBsOff, S.bstart + d.ba, 4u * bc, bar);
+}
+
+// z = U^-1 L^-1 r for the blocks starting in the tile (block_jacobi.wgsl:
+// unit-L forward solve lines 93-101, U backward solve dividing by U(i,i)
+// lines 103-122, rows i < m = min(6, len) only, lines 79 and 124-126). One
+// thread per block, in registers; r from the staged slot 2.
+__device__ __forceinline__ void bj_stage(const UpdDesc &d, const float *stage, float *sz, uint32_t *sflag) {
+    const uint32_t j = threadIdx.x;
+    if (j >= d.nblk) return;
+    const uint32_t *bs = reinterpret_cast<const uint32_t *>(stage + kBsOff);
+    const uint32_t off = bs[d.blk0 + j - d.ba], nxt = bs[d.blk0 + j + 1 - d.ba];
+    const uint32_t m = min(nxt - off, 6u);
+    const float *rr = stage + 2 * kVecCap + (off - d.ra);
+    const float *L = stage + kLuOff + j * 36u;
+    const uint32_t lo = off - d.row0;
+    float y[6], xs[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        y[i] = 0.0f;
+        xs[i] = 0.0f;
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        if ((uint32_t)i < m) {
+            float s = rr[i];
+#pragma unroll
+            for (int q = 0; q < i; ++q) s = __fsub_rn(s, __fmul_rn(L[i * 6 + q], y[q]));
+            y[i] = s;
+        }
+    }
+#pragma unroll
+    for (int i = 5; i >= 0; --i) {
+        if ((uint32_t)i < m) {
+            float s = y[i];
+#pragma unroll
+            for (int q = i + 1; q < 6; ++q)
+                if ((uint32_t)q < m) s = __fsub_rn(s, __fmul_rn(L[i * 6 + q], xs[q]));
+            xs[i] = __fdiv_rn(s, L[i * 6 + i]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+        if ((uint32_t)i < m) {
+            sz[lo + i] = xs[i];
+            sflag[lo + i] = 1u;
+        }
+}
+
+// The last CTA of a system's update tiles (kInit = false, k_update): r.r and
+// r.z from the per-tile partials in tile order, then the host-side logic of
+// compute.rs:466-488 on the device: breakdown checks (pAp == 0, then
+// rz_old == 0), stop test r.r <= abs^2 or r.r <= rel^2 b.b, iteration limit,
+// beta = rz_new / rz_old, residual history entry. kInit = true (k_init):
+// b.b and rz_old; b.b == 0 finishes the system with 0 iterations and x
+// untouched (compute.rs:252-254), max_iter == 0 finishes it as not converged.
+template <bool kInit>
+__device__ __forceinline__ void flush_upd(const SysDesc *__restrict__ sys, StepParams *sp, uint32_t s, uint32_t cnt,
+                                          double *red, int *s_last) {
+    if (cnt == 0) return;
+    const SysDesc &S = sys[s];
+    SysState *st = S.st;
+    if (!take_ticket(&st->cnt_b, cnt, S.n_utiles, s_last)) return;
+    double va = 0.0, vb = 0.0;
+    for (uint32_t i = threadIdx.x; i < S.n_utiles; i += kThreads) {
+        const double2 q = __ldcg(S.part_b + i);
+        va += q.x;
+        vb += q.y;
+    }
+    const double2 sum = block_sum2(va, vb, red);
+    if (threadIdx.x != 0) return;
+    if (kInit) {
+        st->bb = sum.x;
+        st->rz_old = sum.y;
+        uint32_t status = ST_RUNNING;
+        if (sum.x == 0.0) status = ST_CONVERGED;
+        else if (st->max_iter == 0) status = ST_MAXITER;
+        if (status != ST_RUNNING) {
+            st->status = status;
+            st->active = 0;
+            atomicSub(&sp->num_active, 1u);
+        }
+    } else {
+        const double rr_t = sum.x, rz_new = sum.y;
+        const uint32_t it = st->iter;
+        const double pap = st->pap, rz_old = st->rz_old;
+        if (S.history && it < S.hist_cap) S.history[it] = rr_t;
+        st->rr = rr_t;
+        st->rz_new = rz_new;
+        st->iter = it + 1;
+        uint32_t status = ST_RUNNING;
+        if (pap == 0.0) {
+            status = ST_BREAKDOWN;
+            st->breakdown = 1;
+        } else if (rz_old == 0.0) {
+            status = ST_BREAKDOWN;
+            st->breakdown = 2;
+        } else if (rr_t <= st->abs2 || rr_t <= st->rel2 * st->bb) {
+            status = ST_CONVERGED;
+        } else if (it + 1 >= st->max_iter) {
+            status = ST_MAXITER;
+        }
+        const double beta = rz_old != 0.0 ? rz_new / rz_old : 0.0;
+        st->beta = beta;
+        st->beta_f = (float)beta;
+        if (status != ST_RUNNING) {
+            st->status = status;
+            st->active = 0;
+            atomicSub(&sp->num_active, 1u);
+        } else {
+            st->rz_old = rz_new;
+        }
+    }
+    st->cnt_b = 0;
+}
+
+// kInit = false (k_update): x += alpha p; r += (-alpha) Ap; z = M^-1 r; FP64
+// r.r and r.z per tile. kInit = true (k_init, after k_spmv_init):
+// r = b + (-1)(A x0); z = M^-1 r; p = z; FP64 b.b and r.z per tile
+// (compute.rs:226-331). Per-system results are formed by flush_upd.
+template <bool kInit>
+__device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, StepParams *sp, float *smem) {
+    __shared__ __align__(8) uint64_t full[2], empty[2];
+    __shared__ UpdDesc desc[2];
+    __shared__ float sz[kTileRows];
+    __shared__ uint32_t sflag[kTileRows];
+    __shared__ double red[64];
+    __shared__ int s_last, s_ok;
+    const uint32_t tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        mbar_init(&empty[0], kThreads);
+        mbar_init(&empty[1], kThreads);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid >= kThreads) {
+        if (tid != kThreads) return;
+        uint32_t w = blockIdx.x;
+        for (uint32_t k = 0;; ++k) {
+            const uint32_t s = k & 1u;
+            if (k >= 2 && !mbar_wait(&empty[s], ((k >> 1) - 1) & 1u)) {
+                atomicOr(&sp->error, 32u);
+                return;
+            }
+            UpdDesc d;
+            d.valid = resolve_upd<kInit>(sys, sp, &w, &d) ? 1u : 0u;
+            desc[s] = d;
+            if (d.valid) {
+                issue_upd<kInit>(sys, d, smem + s * kUpdStageFloats, &full[s]);
+            } else {
+                mbar_expect_tx(&full[s], 0);
+                return;
+            }
+        }
+    }
+    uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles published since the last ticket
+    for (uint32_t k = 0;; ++k) {
+        const uint32_t s = k & 1u;
+        if (!consumer_wait(&full[s], (k >> 1) & 1u, &s_ok)) {
+            if (tid == 0) {
+                atomicOr(&sp->error, kInit ? 4u : 2u);
+                mbar_wait(&full[s ^ 1u], ((k + 1) >> 1) & 1u);  // bounded drain of the other stage
+            }
+            return;
+        }
+        const UpdDesc d = desc[s];
+        if (!d.valid) break;
+        const SysDesc &S = sys[d.sys];
+        SysState *st = S.st;
+        float *stage = smem + s * kUpdStageFloats;
+        const uint32_t o = d.row0 - d.ra + tid;
+        float ri = 0.0f;
+        double da = 0.0;  // loop: r.r; init: b.b
+        sflag[tid] = 0u;
+        if (tid < d.rows) {
+            const uint32_t i = d.row0 + tid;
+            if (kInit) {
+                const float bi = stage[o];
+                ri = __fsub_rn(bi, stage[3 * kVecCap + o]);
+                da = (double)bi * (double)bi;
+            } else {
+                const float a = st->alpha_f, ma = -a;
+                float xi = stage[o];
+                ri = stage[2 * kVecCap + o];
+                xi = __fadd_rn(xi, __fmul_rn(a, stage[kVecCap + o]));
+                ri = __fadd_rn(ri, __fmul_rn(ma, stage[3 * kVecCap + o]));
+                S.x[i] = xi;
+                da = (double)ri * (double)ri;
+            }
+            S.r[i] = ri;
+            stage[2 * kVecCap + o] = ri;
+        }
+        csync();
+        bj_stage(d, stage, sz, sflag);
+        csync();
+        // The stage is no longer read: hand it back to the producer.
+        fence_proxy_async();
+        mbar_arrive(&empty[s]);
+        double rz = 0.0;
+        if (tid < d.rows) {
+            const uint32_t i = d.row0 + tid;
+            float zi;
+            if (sflag[tid]) {
+                zi = sz[tid];
+                S.z[i] = zi;
+            } else {
+                zi = S.z[i];
+            }
+            if (kInit) S.p[i] = zi;
+            rz = (double)ri * (double)zi;
+        }
+        const double2 tot = block_sum2(da, rz, red);
+        if (d.sys != run_sys) {
+            flush_upd<kInit>(sys, sp, run_sys, run_cnt, red, &s_last);
+            run_sys = d.sys;
+            run_cnt = 0;
+        }
+        if (tid == 0) S.part_b[d.tile] = tot;
+        ++run_cnt;
+    }
+    if (run_sys != 0xffffffffu) flush_upd<kInit>(sys, sp, run_sys, run_cnt, red, &s_last);
 }
 
 }  // namespace
 
-// ---------------------------------------------------------------------------
-// kInit = false: Ap = A p over sp->work_a, FP64 p.Ap; the last CTA of each
-// system sets pAp and alpha = rz_old / pAp (0 when pAp == 0, as
-// pcg_update_scalars.wgsl:59-62).
-// kInit = true: Ap = A x (initial residual) over sp->init_a, no reduction.
-// ---------------------------------------------------------------------------
-template <bool kInit>
-__device__ __forceinline__ void spmv_pass(const SysDesc *__restrict__ sys, StepParams *sp, float *smem) {
-    float *buf = smem;
-    uint32_t *rp = reinterpret_cast<uint32_t *>(smem + kCsrCap + 8);
-    __shared__ double red[64];
-    __shared__ int s_last;
-    const uint32_t nw = kInit ? sp->n_init_a : sp->n_work_a;
-    const WorkItem *__restrict__ work = kInit ? sp->init_a : sp->work_a;
-    for (uint32_t w = blockIdx.x; w < nw; w += gridDim.x) {
-        const WorkItem it = work[w];
-        const SysDesc &S = sys[it.sys];
-        SysState *st = S.st;
-        if (!kInit && !st->active) continue;
-        const SpmvTile T = S.stiles[it.tile];
-        const float *__restrict__ xin = kInit ? S.x : S.p;
-        const TileRows tr = tile_spmv(S, T, xin, buf, rp);
-        const float acc = tr.acc;
-        double part = 0.0;
-        if (threadIdx.x < tr.nrows) {
-            const uint32_t i = tr.row0 + threadIdx.x;
-            S.ap[i] = acc;
-            if (!kInit) part = (double)__ldg(xin + i) * (double)acc;
-        }
-        if (!kInit) {
-            const double tot = block_sum(part, red);
-            if (threadIdx.x == 0) S.part_a[it.tile] = tot;
-            if (take_ticket(&st->cnt_a, S.n_stiles, &s_last)) {
-                double v = 0.0;
-                for (uint32_t i = threadIdx.x; i < S.n_stiles; i += kThreads) v += __ldcg(S.part_a + i);
-                const double pap = block_sum(v, red);
-                if (threadIdx.x == 0) {
-                    const double alpha = pap != 0.0 ? st->rz_old / pap : 0.0;
-                    st->pap = pap;
-                    st->alpha = alpha;
-                    st->alpha_f = (float)alpha;
-                    st->cnt_a = 0;
-                }
-            }
-        }
-        __syncthreads();
-    }
-}
-__global__ void __launch_bounds__(kThreads) k_spmv_loop(const SysDesc *__restrict__ sys, StepParams *sp) {
-    extern __shared__ __align__(16) float smem[];
-    spmv_pass<false>(sys, sp, smem);
+__global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_loop(const SysDesc *__restrict__ sys, StepParams *sp) {
+    extern __shared__ __align__(128) float smem[];
+    spmv_pipeline<M_LOOP>(sys, sp, nullptr, nullptr, smem);
 }
 
-__global__ void __launch_bounds__(kThreads) k_spmv_init(const SysDesc *__restrict__ sys, StepParams *sp) {
-    extern __shared__ __align__(16) float smem[];
-    spmv_pass<true>(sys, sp, smem);
+__global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_init(const SysDesc *__restrict__ sys, StepParams *sp) {
+    extern __shared__ __align__(128) float smem[];
+    spmv_pipeline<M_INIT>(sys, sp, nullptr, nullptr, smem);
+}
+
+__global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_plain(const SysDesc *__restrict__ sys, StepParams *sp,
+                                                         const float *__restrict__ x, float *__restrict__ y) {
+    extern __shared__ __align__(128) float smem[];
+    spmv_pipeline<M_PLAIN>(sys, sp, x, y, smem);
+}
+
+__global__ void __launch_bounds__(kPipeThreads, 4) k_update(const SysDesc *__restrict__ sys, StepParams *sp) {
+    extern __shared__ __align__(128) float smem[];
+    upd_pipeline<false>(sys, sp, smem);
+}
+
+__global__ void __launch_bounds__(kPipeThreads, 4) k_init(const SysDesc *__restrict__ sys, StepParams *sp) {
+    extern __shared__ __align__(128) float smem[];
+    upd_pipeline<true>(sys, sp, smem);
 }
 
 // ---------------------------------------------------------------------------
-// k_update: x += alpha p; r += (-alpha) Ap; z = M^-1 r; FP64 r.r and r.z.
-// The last CTA of a system runs the host-side logic of compute.rs:466-488 on
-// the device: breakdown checks (pAp == 0, then rz_old == 0), the stop test
-// r.r <= abs^2 or r.r <= rel^2 * b.b, the iteration limit, beta = rz_new /
-// rz_old, and the residual history entry.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_update(const SysDesc *__restrict__ sys, StepParams *sp) {
-    __shared__ float sr[kTileRows], sz[kTileRows];
-    __shared__ uint32_t sflag[kTileRows];
-    __shared__ __align__(16) float slu[kLuStage * 36];
-    __shared__ double red[64];
-    __shared__ int s_last;
-    const uint32_t nw = sp->n_work_b;
-    const WorkItem *__restrict__ work = sp->work_b;
-    const uint32_t t = threadIdx.x;
-    for (uint32_t w = blockIdx.x; w < nw; w += gridDim.x) {
-        const WorkItem it = work[w];
-        const SysDesc &S = sys[it.sys];
-        SysState *st = S.st;
-        if (!st->active) continue;
-        const UpdTile T = S.utiles[it.tile];
-        const float a = st->alpha_f, ma = -a;
-        const uint32_t rows = T.row1 - T.row0;
-        float ri = 0.0f;
-        double rr = 0.0;
-        sflag[t] = 0u;
-        if (t < rows) {
-            const uint32_t i = T.row0 + t;
-            const float pi = S.p[i], api = S.ap[i];
-            float xi = S.x[i];
-            ri = S.r[i];
-            xi = __fadd_rn(xi, __fmul_rn(a, pi));
-            ri = __fadd_rn(ri, __fmul_rn(ma, api));
-            S.x[i] = xi;
-            S.r[i] = ri;
-            sr[t] = ri;
-            rr = (double)ri * (double)ri;
-        }
-        __syncthreads();
-        bj_tile(S, T, sr, sz, sflag, slu);
-        double rz = 0.0;
-        if (t < rows) {
-            const uint32_t i = T.row0 + t;
-            float zi;
-            if (sflag[t]) {
-                zi = sz[t];
-                S.z[i] = zi;
-            } else {
-                zi = S.z[i];
-            }
-            rz = (double)ri * (double)zi;
-        }
-        const double2 tot = block_sum2(rr, rz, red);
-        if (t == 0) S.part_b[it.tile] = tot;
-        if (take_ticket(&st->cnt_b, S.n_utiles, &s_last)) {
-            double va = 0.0, vb = 0.0;
-            for (uint32_t i = t; i < S.n_utiles; i += kThreads) {
-                const double2 q = __ldcg(S.part_b + i);
-                va += q.x;
-                vb += q.y;
-            }
-            const double2 sum = block_sum2(va, vb, red);
-            if (t == 0) {
-                const double rr_t = sum.x, rz_new = sum.y;
-                const uint32_t k = st->iter;
-                const double pap = st->pap, rz_old = st->rz_old;
-                if (S.history && k < S.hist_cap) S.history[k] = rr_t;
-                st->rr = rr_t;
-                st->rz_new = rz_new;
-                st->iter = k + 1;
-                uint32_t status = ST_RUNNING;
-                if (pap == 0.0) {
-                    status = ST_BREAKDOWN;
-                    st->breakdown = 1;
-                } else if (rz_old == 0.0) {
-                    status = ST_BREAKDOWN;
-                    st->breakdown = 2;
-                } else if (rr_t <= st->abs2 || rr_t <= st->rel2 * st->bb) {
-                    status = ST_CONVERGED;
-                } else if (k + 1 >= st->max_iter) {
-                    status = ST_MAXITER;
-                }
-                const double beta = rz_old != 0.0 ? rz_new / rz_old : 0.0;
-                st->beta = beta;
-                st->beta_f = (float)beta;
-                if (status != ST_RUNNING) {
-                    st->status = status;
-                    st->active = 0;
-                    atomicSub(&sp->num_active, 1u);
-                } else {
-                    st->rz_old = rz_new;
-                }
-                st->cnt_b = 0;
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// ---------------------------------------------------------------------------
-// k_init (after k_spmv<true>): r = b + (-1)(A x0); z = M^-1 r; p = z;
-// FP64 b.b and r.z (compute.rs:226-331). The last CTA stores b.b and rz_old;
-// b.b == 0 finishes the system with 0 iterations and x untouched
-// (compute.rs:252-254); max_iter == 0 finishes it as not converged.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_init(const SysDesc *__restrict__ sys, StepParams *sp) {
-    __shared__ float sr[kTileRows], sz[kTileRows];
-    __shared__ uint32_t sflag[kTileRows];
-    __shared__ __align__(16) float slu[kLuStage * 36];
-    __shared__ double red[64];
-    __shared__ int s_last;
-    const uint32_t nw = sp->n_init_b;
-    const WorkItem *__restrict__ work = sp->init_b;
-    const uint32_t t = threadIdx.x;
-    for (uint32_t w = blockIdx.x; w < nw; w += gridDim.x) {
-        const WorkItem it = work[w];
-        const SysDesc &S = sys[it.sys];
-        SysState *st = S.st;
-        const UpdTile T = S.utiles[it.tile];
-        const uint32_t rows = T.row1 - T.row0;
-        float ri = 0.0f;
-        double bb = 0.0;
-        sflag[t] = 0u;
-        if (t < rows) {
-            const uint32_t i = T.row0 + t;
-            const float bi = S.b[i];
-            ri = __fsub_rn(bi, S.ap[i]);
-            S.r[i] = ri;
-            sr[t] = ri;
-            bb = (double)bi * (double)bi;
-        }
-        __syncthreads();
-        bj_tile(S, T, sr, sz, sflag, slu);
-        double rz = 0.0;
-        if (t < rows) {
-            const uint32_t i = T.row0 + t;
-            float zi;
-            if (sflag[t]) {
-                zi = sz[t];
-                S.z[i] = zi;
-            } else {
-                zi = S.z[i];
-            }
-            S.p[i] = zi;
-            rz = (double)ri * (double)zi;
-        }
-        const double2 tot = block_sum2(bb, rz, red);
-        if (t == 0) S.part_b[it.tile] = tot;
-        if (take_ticket(&st->cnt_b, S.n_utiles, &s_last)) {
-            double va = 0.0, vb = 0.0;
-            for (uint32_t i = t; i < S.n_utiles; i += kThreads) {
-                const double2 q = __ldcg(S.part_b + i);
-                va += q.x;
-                vb += q.y;
-            }
-            const double2 sum = block_sum2(va, vb, red);
-            if (t == 0) {
-                st->bb = sum.x;
-                st->rz_old = sum.y;
-                uint32_t status = ST_RUNNING;
-                if (sum.x == 0.0) status = ST_CONVERGED;
-                else if (st->max_iter == 0) status = ST_MAXITER;
-                if (status != ST_RUNNING) {
-                    st->status = status;
-                    st->active = 0;
-                    atomicSub(&sp->num_active, 1u);
-                }
-                st->cnt_b = 0;
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// ---------------------------------------------------------------------------
-// k_pupdate: p = p*beta + z (scale_from_scalar_results.wgsl then axpy.wgsl
-// with alpha 1). CTA 0 then ends the graph's while loop when no system is
-// active or the step's iteration budget is used.
+// k_pupdate: p = p*beta + z over kChunkRows row chunks with float4 accesses
+// (scale_from_scalar_results.wgsl then axpy.wgsl with alpha 1). CTA 0 then
+// ends the graph's while loop when no system is active, the step's iteration
+// budget is used, or a kernel reported an error.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kThreads) k_pupdate(const SysDesc *__restrict__ sys, StepParams *sp,
                                                       cudaGraphConditionalHandle h) {
-    const uint32_t nw = sp->n_work_b;
-    const WorkItem *__restrict__ work = sp->work_b;
+    const uint32_t nw = sp->n_work_c;
+    const WorkItem *__restrict__ work = sp->work_c;
     for (uint32_t w = blockIdx.x; w < nw; w += gridDim.x) {
         const WorkItem it = work[w];
+        if (it.sys >= sp->num_sys || it.tile * (uint32_t)kChunkRows >= sys[it.sys].n) {
+            if (threadIdx.x == 0) atomicOr(&sp->error, 8u);
+            continue;
+        }
         const SysDesc &S = sys[it.sys];
         const SysState *st = S.st;
         if (!st->active) continue;
-        const UpdTile T = S.utiles[it.tile];
         const float bf = st->beta_f;
-        const uint32_t rows = T.row1 - T.row0;
-        if (threadIdx.x < rows) {
-            const uint32_t i = T.row0 + threadIdx.x;
-            S.p[i] = __fadd_rn(__fmul_rn(S.p[i], bf), S.z[i]);
+        const uint32_t r0 = it.tile * (uint32_t)kChunkRows;
+        const uint32_t r1 = min(S.n, r0 + (uint32_t)kChunkRows);
+        float *__restrict__ p = S.p;
+        const float *__restrict__ z = S.z;
+        uint32_t q = r0 + 4u * threadIdx.x;
+        for (; q + 4u * kThreads + 3u < r1; q += 8u * kThreads) {
+            float4 p0 = *reinterpret_cast<const float4 *>(p + q);
+            float4 p1 = *reinterpret_cast<const float4 *>(p + q + 4u * kThreads);
+            const float4 z0 = *reinterpret_cast<const float4 *>(z + q);
+            const float4 z1 = *reinterpret_cast<const float4 *>(z + q + 4u * kThreads);
+            p0.x = __fadd_rn(__fmul_rn(p0.x, bf), z0.x);
+            p0.y = __fadd_rn(__fmul_rn(p0.y, bf), z0.y);
+            p0.z = __fadd_rn(__fmul_rn(p0.z, bf), z0.z);
+            p0.w = __fadd_rn(__fmul_rn(p0.w, bf), z0.w);
+            p1.x = __fadd_rn(__fmul_rn(p1.x, bf), z1.x);
+            p1.y = __fadd_rn(__fmul_rn(p1.y, bf), z1.y);
+            p1.z = __fadd_rn(__fmul_rn(p1.z, bf), z1.z);
+            p1.w = __fadd_rn(__fmul_rn(p1.w, bf), z1.w);
+            *reinterpret_cast<float4 *>(p + q) = p0;
+            *reinterpret_cast<float4 *>(p + q + 4u * kThreads) = p1;
+        }
+        for (; q < r1; q += 4u * kThreads) {
+            if (q + 3u < r1) {
+                float4 p0 = *reinterpret_cast<const float4 *>(p + q);
+                const float4 z0 = *reinterpret_cast<const float4 *>(z + q);
+                p0.x = __fadd_rn(__fmul_rn(p0.x, bf), z0.x);
+                p0.y = __fadd_rn(__fmul_rn(p0.y, bf), z0.y);
+                p0.z = __fadd_rn(__fmul_rn(p0.z, bf), z0.z);
+                p0.w = __fadd_rn(__fmul_rn(p0.w, bf), z0.w);
+                *reinterpret_cast<float4 *>(p + q) = p0;
+            } else {
+                for (uint32_t i = q; i < r1; ++i) p[i] = __fadd_rn(__fmul_rn(p[i], bf), z[i]);
+            }
         }
     }
     if (h != 0 && blockIdx.x == 0 && threadIdx.x == 0) {
         const uint32_t c = sp->loop_count + 1;
         sp->loop_count = c;
-        if (sp->num_active == 0 || c >= sp->loop_limit) cudaGraphSetConditional(h, 0);
+        if (sp->num_active == 0 || c >= sp->loop_limit || sp->error != 0) cudaGraphSetConditional(h, 0);
     }
 }
 
@@ -520,7 +852,7 @@ __global__ void __launch_bounds__(kThreads) k_pupdate(const SysDesc *__restrict_
 __global__ void k_loop_gate(StepParams *sp, cudaGraphConditionalHandle h) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         sp->loop_count = 0;
-        cudaGraphSetConditional(h, (sp->num_active > 0 && sp->loop_limit > 0) ? 1u : 0u);
+        cudaGraphSetConditional(h, (sp->num_active > 0 && sp->loop_limit > 0 && sp->error == 0) ? 1u : 0u);
     }
 }
 
@@ -537,6 +869,10 @@ __global__ void __launch_bounds__(kThreads) k_resid64(const SysDesc *__restrict_
     const uint32_t t = threadIdx.x;
     for (uint32_t w = blockIdx.x; w < nw; w += gridDim.x) {
         const WorkItem it = work[w];
+        if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_utiles) {
+            if (threadIdx.x == 0) atomicOr(&sp->error, 8u);
+            continue;
+        }
         const SysDesc &S = sys[it.sys];
         SysState *st = S.st;
         const UpdTile T = S.utiles[it.tile];
@@ -565,7 +901,7 @@ __global__ void __launch_bounds__(kThreads) k_resid64(const SysDesc *__restrict_
         }
         const double2 tot = block_sum2(rr, bb, red);
         if (t == 0) S.part_b[it.tile] = tot;
-        if (take_ticket(&st->cnt_c, S.n_utiles, &s_last)) {
+        if (take_ticket(&st->cnt_c, 1u, S.n_utiles, &s_last)) {
             double va = 0.0, vb = 0.0;
             for (uint32_t i = t; i < S.n_utiles; i += kThreads) {
                 const double2 q = __ldcg(S.part_b + i);
@@ -579,7 +915,7 @@ __global__ void __launch_bounds__(kThreads) k_resid64(const SysDesc *__restrict_
                 st->cnt_c = 0;
             }
         }
-        __syncthreads();
+        csync();
     }
 }
 
@@ -589,6 +925,10 @@ __global__ void __launch_bounds__(kThreads) k_refine(const SysDesc *__restrict__
     const WorkItem *__restrict__ work = sp->aux_b;
     for (uint32_t w = blockIdx.x; w < nw; w += gridDim.x) {
         const WorkItem it = work[w];
+        if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_utiles) {
+            if (threadIdx.x == 0) atomicOr(&sp->error, 8u);
+            continue;
+        }
         const SysDesc &S = sys[it.sys];
         const UpdTile T = S.utiles[it.tile];
         if (threadIdx.x < T.row1 - T.row0) {
@@ -605,27 +945,16 @@ __global__ void __launch_bounds__(kThreads) k_x64_to_x32(const SysDesc *__restri
     const WorkItem *__restrict__ work = sp->aux_b;
     for (uint32_t w = blockIdx.x; w < nw; w += gridDim.x) {
         const WorkItem it = work[w];
+        if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_utiles) {
+            if (threadIdx.x == 0) atomicOr(&sp->error, 8u);
+            continue;
+        }
         const SysDesc &S = sys[it.sys];
         const UpdTile T = S.utiles[it.tile];
         if (threadIdx.x < T.row1 - T.row0) {
             const uint32_t i = T.row0 + threadIdx.x;
             S.x[i] = (float)S.x64[i];
         }
-    }
-}
-
-// y = A x over all SpMV tiles of one system (no reduction).
-__global__ void __launch_bounds__(kThreads) k_spmv_plain(const SysDesc *__restrict__ sys, const float *__restrict__ x,
-                                                         float *__restrict__ y) {
-    extern __shared__ __align__(16) float smem[];
-    float *buf = smem;
-    uint32_t *rp = reinterpret_cast<uint32_t *>(smem + kCsrCap + 8);
-    const SysDesc &S = sys[0];
-    for (uint32_t w = blockIdx.x; w < S.n_stiles; w += gridDim.x) {
-        const SpmvTile T = S.stiles[w];
-        const TileRows tr = tile_spmv(S, T, x, buf, rp);
-        if (threadIdx.x < tr.nrows) y[tr.row0 + threadIdx.x] = tr.acc;
-        __syncthreads();
     }
 }
 

@@ -17,8 +17,15 @@
 
 namespace wsb {
 
-// Bytes of dynamic shared memory used by k_spmv.
-constexpr size_t kSpmvSmem = (size_t)kCsrCap * sizeof(float) + (kTileRows + 8) * sizeof(uint32_t);
+// Shared-memory stages (floats) of the two TMA-pipelined kernels; each
+// kernel double-buffers its stage.
+constexpr int kSpmvStageFloats = ((2 * (kCsrCap + 8) + kTileRows + 8) + 31) & ~31;
+constexpr int kUpdStageFloats = ((4 * (kTileRows + 8) + kUpdBlocks * 36 + kUpdBlocks + 8) + 31) & ~31;
+// Threads per CTA of the TMA-pipelined kernels: kThreads consumers plus one
+// producer warp.
+constexpr int kPipeThreads = kThreads + 32;
+constexpr size_t kSpmvSmem = 2 * (size_t)kSpmvStageFloats * sizeof(float);
+constexpr size_t kUpdSmem = 2 * (size_t)kUpdStageFloats * sizeof(float);
 
 // k_spmv_loop: Ap = A p with p.Ap and alpha; k_spmv_init: Ap = A x.
 __global__ void k_spmv_loop(const SysDesc *__restrict__ sys, StepParams *sp);
@@ -33,7 +40,9 @@ __global__ void k_resid64(const SysDesc *__restrict__ sys, StepParams *sp);
 __global__ void k_refine(const SysDesc *__restrict__ sys, StepParams *sp);
 __global__ void k_x64_to_x32(const SysDesc *__restrict__ sys, StepParams *sp);
 
-// Plain y = A x of one system over its own tiles (no reduction).
-__global__ void k_spmv_plain(const SysDesc *__restrict__ sys, const float *__restrict__ x, float *__restrict__ y);
+// Plain y = A x of one system (sys[0]) over its own tiles (no reduction);
+// sp receives the error code of a timed-out wait.
+__global__ void k_spmv_plain(const SysDesc *__restrict__ sys, StepParams *sp, const float *__restrict__ x,
+                             float *__restrict__ y);
 
 }  // namespace wsb

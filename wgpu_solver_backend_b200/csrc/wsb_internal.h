@@ -21,9 +21,10 @@ namespace wsb {
 // ---------------------------------------------------------------------------
 constexpr int kThreads = 256;        // threads per CTA for every solver kernel
 constexpr int kTileRows = 256;       // rows (or block rows x 6) per tile, <= kThreads
-constexpr int kCsrCap = 12288;       // CSR nonzeros staged in shared memory per chunk
-constexpr int kBsrCapBlocks = 256;   // BSR 6x6 blocks staged per chunk (36 KiB of values)
-constexpr int kLuStage = 64;         // LU blocks staged in shared memory per pass
+constexpr int kCsrCap = 6144;        // CSR nonzeros per SpMV tile (one TMA stage)
+constexpr int kBsrCapBlocks = 256;   // BSR 6x6 blocks per SpMV tile (36 KiB of values)
+constexpr int kUpdBlocks = 64;       // block-Jacobi blocks per update tile
+constexpr int kChunkRows = 4096;     // rows per work item of the vector kernels
 constexpr int kPadElems = 64;        // tail padding of streamed arrays (elements)
 
 enum SysStatus : uint32_t {
@@ -35,12 +36,15 @@ enum SysStatus : uint32_t {
 
 enum Layout : uint32_t { LAYOUT_CSR = 1, LAYOUT_BSR6 = 2 };
 
-// Row tile of the SpMV: rows [row0, row1) (CSR) or block rows (BSR6).
+// Row tile of the SpMV: rows [row0, row1) (CSR) or block rows (BSR6), and
+// their nonzero (or 6x6 block) range [k0, k1). A tile holds at most
+// kCsrCap nonzeros (kBsrCapBlocks blocks) unless it is a single longer row.
 struct SpmvTile {
-    uint32_t row0, row1;
+    uint32_t row0, row1, k0, k1;
 };
-// Row tile of the update kernels; never cuts the first 6 rows of a block.
-// Blocks whose first row lies in [row0, row1) are [blk0, blk1).
+// Row tile of the update kernels; never cuts the first 6 rows of a block and
+// holds at most kUpdBlocks block starts. Blocks whose first row lies in
+// [row0, row1) are [blk0, blk1).
 struct UpdTile {
     uint32_t row0, row1, blk0, blk1;
 };
@@ -89,15 +93,19 @@ struct SysDesc {
 struct StepParams {
     const WorkItem *work_a;            // loop: SpMV tiles of active systems
     const WorkItem *work_b;            // loop: update tiles of active systems
+    const WorkItem *work_c;            // loop: kChunkRows row chunks of active systems
     const WorkItem *init_a;            // init: SpMV tiles of systems (re)starting
     const WorkItem *init_b;            // init: update tiles of systems (re)starting
     const WorkItem *aux_b;             // refinement kernels: update tiles
-    uint32_t n_work_a, n_work_b;
+    uint32_t n_work_a, n_work_b, n_work_c;
     uint32_t n_init_a, n_init_b;
     uint32_t n_aux_b;
     uint32_t num_active;               // systems still iterating
     uint32_t loop_count;               // body executions in this launch
     uint32_t loop_limit;               // stop the while loop after this many
+    uint32_t error;                    // nonzero: a bounded wait ran out or a work item was invalid
+    uint32_t num_sys;                  // entries of the SysDesc array (work items are checked against it)
+    uint32_t pad;
 };
 
 // ---------------------------------------------------------------------------
