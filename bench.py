@@ -263,7 +263,10 @@ def run_kernels(args, world, rank, local):
                           layout=wsb.LAYOUT_CSR if args.layout == "csr" else wsb.LAYOUT_AUTO)
     d_b = torch.from_numpy(s["b"]).cuda()
     torch.cuda.synchronize()
-    kt = m.kernel_times(d_b.data_ptr(), iterations=args.iters)
+    try:
+        kt = m.kernel_times(d_b.data_ptr(), iterations=args.iters)
+    except Exception as e:  # report instead of a bogus timing
+        return {"workload": f"kernels: {args.side}^3", "error": str(e)}
     info = m.info
     peak, kind = peaks()
     out = {"workload": f"kernels: {args.side}^3 lattice, n={s['n']}, layout {args.layout}", "iterations": args.iters,

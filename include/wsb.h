@@ -250,7 +250,9 @@ int wsb_matrix_spmv_device(wsb_context *ctx, wsb_matrix *m, const float *d_x, fl
  * iterations of this matrix with right-hand side d_b (device) outside the
  * CUDA graph, CUDA events around each launch, and writes the mean duration
  * in ms of the SpMV+p.Ap kernel, the update+preconditioner kernel and the
- * p-update kernel to ms[0..2]. */
+ * p-update kernel to ms[0..2]; ms[3] and ms[4] receive the iteration count
+ * and status code of the system afterwards (a valid measurement has
+ * ms[3] == iterations and status 0, still running). ms holds 5 doubles. */
 int wsb_matrix_kernel_times(wsb_context *ctx, wsb_matrix *m, const float *d_b, uint32_t iterations, double *ms);
 
 /* ------------------------------------------------------------------------- */

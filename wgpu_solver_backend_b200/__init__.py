@@ -404,9 +404,12 @@ class Matrix:
 
     def kernel_times(self, d_b: int, iterations: int = 20) -> dict:
         """Mean per-launch device time (ms) of the three loop kernels."""
-        ms = np.zeros(3, np.float64)
+        ms = np.zeros(5, np.float64)
         _check(_lib_handle().wsb_matrix_kernel_times(self.ctx.handle, self.handle, C.c_void_p(d_b), int(iterations),
                                                      _p(ms, _lib.f64p)), self.ctx.handle)
+        if int(ms[3]) != int(iterations) or int(ms[4]) != 0:
+            raise WsbError(_lib.CUDA, f"kernel timing invalid: system stopped after {int(ms[3])} of {iterations} "
+                                      f"iterations (status {int(ms[4])})")
         return dict(spmv_ms=ms[0], update_ms=ms[1], pupdate_ms=ms[2])
 
     def spmv_device(self, d_x: int, d_y: int):

@@ -715,7 +715,7 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
     return WSB_OK;
 }
 
-int Engine::profile_kernels(uint32_t s, uint32_t iters, double ms[3]) {
+int Engine::profile_kernels(uint32_t s, uint32_t iters, double ms[5]) {
     int rc;
     Slot &sl = *slots_[s];
     if (sl.A->n == 0 || iters == 0) return fail(ctx_, WSB_ERR_BAD_INPUT, "nothing to profile");
@@ -768,6 +768,12 @@ int Engine::profile_kernels(uint32_t s, uint32_t iters, double ms[3]) {
         }
     for (auto &e : ev) cudaEventDestroy(e);
     for (int k = 0; k < 3; ++k) ms[k] = acc[k] / iters;
+    // The system must still be iterating after `iters` iterations, or the
+    // later launches did no work and the means above are not kernel times.
+    WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(h_state_ + s, d_state_ + s, sizeof(SysState), cudaMemcpyDeviceToHost, stream_));
+    WSB_CUDA_TRY(ctx_, cudaStreamSynchronize(stream_));
+    ms[3] = (double)h_state_[s].iter;
+    ms[4] = (double)h_state_[s].status;
     sl.phase = Slot::DONE;
     work_dirty_ = true;
     return WSB_OK;

@@ -84,8 +84,9 @@ class Engine {
     int reset_slot(uint32_t slot, const SolveCfg &cfg);  // reuse for another solve
     // Runs the init kernels and then `iters` loop iterations of one slot
     // outside the graph with CUDA events around every launch; ms[0..2] get
-    // the mean duration of k_spmv_loop, k_update and k_pupdate.
-    int profile_kernels(uint32_t slot, uint32_t iters, double ms[3]);
+    // the mean duration of k_spmv_loop, k_update and k_pupdate; ms[3] and
+    // ms[4] the system's iteration count and status afterwards.
+    int profile_kernels(uint32_t slot, uint32_t iters, double ms[5]);
     void remove(uint32_t slot);
     bool done(uint32_t slot) const;
     uint64_t slot_bytes(uint32_t slot) const;

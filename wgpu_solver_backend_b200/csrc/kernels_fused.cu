@@ -167,7 +167,7 @@ enum SpmvMode { M_LOOP = 0, M_INIT = 1, M_PLAIN = 2 };
 constexpr int kValCap = kCsrCap + 8;
 constexpr int kColOff = kValCap;
 constexpr int kBcolOff = kBsrCapBlocks * 36;
-constexpr int kRpOff = 2 * kValCap;
+constexpr int kRpOff = kSpmvRpOff;
 constexpr int kXgOff = kBcolOff + kBsrCapBlocks + 8;  // BSR6: gathered x, 6 per block
 static_assert(kXgOff + 6 * kBsrCapBlocks <= kRpOff, "BSR stage fits");
 static_assert((kColOff * 4) % 16 == 0 && (kBcolOff * 4) % 16 == 0 && (kRpOff * 4) % 16 == 0, "TMA alignment");
@@ -258,13 +258,12 @@ __device__ __forceinline__ float csr_stage(const SpmvDesc &d, const float *__res
     const uint32_t *rp = reinterpret_cast<const uint32_t *>(stage + kRpOff);
     const uint32_t j0 = d.k0 - d.ka, j1 = d.k1 - d.ka;
     uint32_t j = j0 + threadIdx.x;
-    for (; j + 3 * kThreads < j1; j += 4 * kThreads) {
-        const uint32_t c0 = col[j], c1 = col[j + kThreads], c2 = col[j + 2 * kThreads], c3 = col[j + 3 * kThreads];
-        const float x0 = __ldg(xin + c0), x1 = __ldg(xin + c1), x2 = __ldg(xin + c2), x3 = __ldg(xin + c3);
-        val[j] = __fmul_rn(val[j], x0);
-        val[j + kThreads] = __fmul_rn(val[j + kThreads], x1);
-        val[j + 2 * kThreads] = __fmul_rn(val[j + 2 * kThreads], x2);
-        val[j + 3 * kThreads] = __fmul_rn(val[j + 3 * kThreads], x3);
+    for (; j + 7 * kThreads < j1; j += 8 * kThreads) {
+        float xv[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) xv[q] = __ldg(xin + col[j + q * kThreads]);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) val[j + q * kThreads] = __fmul_rn(val[j + q * kThreads], xv[q]);
     }
     for (; j < j1; j += kThreads) val[j] = __fmul_rn(val[j], __ldg(xin + col[j]));
     csync();
@@ -288,19 +287,19 @@ __device__ __forceinline__ float bsr_stage(const SpmvDesc &d, const float *__res
     float *xg = stage + kXgOff;
     const uint32_t nb = d.k1 - d.k0, cofs = d.k0 - d.ka;
     const uint32_t ne = 6u * nb;
-    uint32_t e = threadIdx.x;
-    for (; e + 3 * kThreads < ne; e += 4 * kThreads) {
-        const uint32_t e1 = e + kThreads, e2 = e + 2 * kThreads, e3 = e + 3 * kThreads;
-        const float v0 = __ldg(xin + 6u * (size_t)bcol[e / 6u + cofs] + e % 6u);
-        const float v1 = __ldg(xin + 6u * (size_t)bcol[e1 / 6u + cofs] + e1 % 6u);
-        const float v2 = __ldg(xin + 6u * (size_t)bcol[e2 / 6u + cofs] + e2 % 6u);
-        const float v3 = __ldg(xin + 6u * (size_t)bcol[e3 / 6u + cofs] + e3 % 6u);
-        xg[e] = v0;
-        xg[e1] = v1;
-        xg[e2] = v2;
-        xg[e3] = v3;
+    // Up to kGather independent loads per thread in flight at once.
+    constexpr int kGather = (6 * kBsrCapBlocks + kThreads - 1) / kThreads;
+    float v[kGather];
+#pragma unroll
+    for (int q = 0; q < kGather; ++q) {
+        const uint32_t e = threadIdx.x + q * kThreads;
+        v[q] = e < ne ? __ldg(xin + 6u * (size_t)bcol[e / 6u + cofs] + e % 6u) : 0.0f;
     }
-    for (; e < ne; e += kThreads) xg[e] = __ldg(xin + 6u * (size_t)bcol[e / 6u + cofs] + e % 6u);
+#pragma unroll
+    for (int q = 0; q < kGather; ++q) {
+        const uint32_t e = threadIdx.x + q * kThreads;
+        if (e < ne) xg[e] = v[q];
+    }
     csync();
     float acc = 0.0f;
     const uint32_t t = threadIdx.x;
@@ -436,12 +435,14 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
         float *stage = smem + s * kSpmvStageFloats;
         const SysDesc &S = sys[d.sys];
         const float *__restrict__ xin = kMode == M_PLAIN ? xplain : kMode == M_INIT ? S.x : S.p;
+        const uint32_t row0 = d.layout == LAYOUT_BSR6 ? 6u * d.r0 : d.r0;
+        const uint32_t nrows = d.layout == LAYOUT_BSR6 ? 6u * d.nr : d.nr;
+        // p(i) of this thread's row for p.Ap, loaded ahead of the tile's work.
+        const float p_own = (kMode == M_LOOP && tid < nrows) ? __ldg(xin + row0 + tid) : 0.0f;
         float acc;
         if (d.lng) acc = long_tile(S, d, xin, stage);
         else if (d.layout == LAYOUT_BSR6) acc = bsr_stage(d, xin, stage);
         else acc = csr_stage(d, xin, stage);
-        const uint32_t row0 = d.layout == LAYOUT_BSR6 ? 6u * d.r0 : d.r0;
-        const uint32_t nrows = d.layout == LAYOUT_BSR6 ? 6u * d.nr : d.nr;
         // Everyone is done reading the stage: hand it back to the producer.
         fence_proxy_async();
         mbar_arrive(&empty[s]);
@@ -452,7 +453,7 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
             if (tid < nrows) {
                 const uint32_t i = row0 + tid;
                 S.ap[i] = acc;
-                if (kMode == M_LOOP) part = (double)__ldg(xin + i) * (double)acc;
+                if (kMode == M_LOOP) part = (double)p_own * (double)acc;
             }
             if (kMode == M_LOOP) {
                 const double tot = block_sum(part, red);
@@ -482,7 +483,8 @@ struct UpdDesc {
     uint32_t valid, sys, tile;
     uint32_t row0, rows, blk0, nblk;
     uint32_t ra, ba;  // 4-aligned starts of the staged row / block-start ranges
-    uint32_t pad[3];
+    float alpha;      // the system's alpha (loop kernel), read by the producer
+    uint32_t pad[2];
 };
 
 template <bool kInit>
@@ -508,6 +510,7 @@ __device__ __forceinline__ bool resolve_upd(const SysDesc *__restrict__ sys, con
         d->nblk = T.blk1 - T.blk0;
         d->ra = T.row0 & ~3u;
         d->ba = T.blk0 & ~3u;
+        d->alpha = kInit ? 0.0f : sys[it.sys].st->alpha_f;
         return true;
     }
 }
@@ -702,7 +705,6 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
         const UpdDesc d = desc[s];
         if (!d.valid) break;
         const SysDesc &S = sys[d.sys];
-        SysState *st = S.st;
         float *stage = smem + s * kUpdStageFloats;
         const uint32_t o = d.row0 - d.ra + tid;
         float ri = 0.0f;
@@ -715,7 +717,7 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
                 ri = __fsub_rn(bi, stage[3 * kVecCap + o]);
                 da = (double)bi * (double)bi;
             } else {
-                const float a = st->alpha_f, ma = -a;
+                const float a = d.alpha, ma = -a;
                 float xi = stage[o];
                 ri = stage[2 * kVecCap + o];
                 xi = __fadd_rn(xi, __fmul_rn(a, stage[kVecCap + o]));
@@ -759,17 +761,17 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
 
 }  // namespace
 
-__global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_loop(const SysDesc *__restrict__ sys, StepParams *sp) {
+__global__ void __launch_bounds__(kPipeThreads, 3) k_spmv_loop(const SysDesc *__restrict__ sys, StepParams *sp) {
     extern __shared__ __align__(128) float smem[];
     spmv_pipeline<M_LOOP>(sys, sp, nullptr, nullptr, smem);
 }
 
-__global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_init(const SysDesc *__restrict__ sys, StepParams *sp) {
+__global__ void __launch_bounds__(kPipeThreads, 3) k_spmv_init(const SysDesc *__restrict__ sys, StepParams *sp) {
     extern __shared__ __align__(128) float smem[];
     spmv_pipeline<M_INIT>(sys, sp, nullptr, nullptr, smem);
 }
 
-__global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_plain(const SysDesc *__restrict__ sys, StepParams *sp,
+__global__ void __launch_bounds__(kPipeThreads, 3) k_spmv_plain(const SysDesc *__restrict__ sys, StepParams *sp,
                                                          const float *__restrict__ x, float *__restrict__ y) {
     extern __shared__ __align__(128) float smem[];
     spmv_pipeline<M_PLAIN>(sys, sp, x, y, smem);

@@ -19,7 +19,12 @@ namespace wsb {
 
 // Shared-memory stages (floats) of the two TMA-pipelined kernels; each
 // kernel double-buffers its stage.
-constexpr int kSpmvStageFloats = ((2 * (kCsrCap + 8) + kTileRows + 8) + 31) & ~31;
+// SpMV stage: CSR values + columns, or BSR6 block values + block columns +
+// gathered x, then the row pointers at kSpmvRpOff.
+constexpr int kSpmvDataFloats = (2 * (kCsrCap + 8) > 43 * kBsrCapBlocks + 8) ? 2 * (kCsrCap + 8)
+                                                                             : 43 * kBsrCapBlocks + 8;
+constexpr int kSpmvRpOff = (kSpmvDataFloats + 3) & ~3;
+constexpr int kSpmvStageFloats = ((kSpmvRpOff + kTileRows + 8) + 31) & ~31;
 constexpr int kUpdStageFloats = ((4 * (kTileRows + 8) + kUpdBlocks * 36 + kUpdBlocks + 8) + 31) & ~31;
 // Threads per CTA of the TMA-pipelined kernels: kThreads consumers plus one
 // producer warp.

@@ -21,8 +21,8 @@ namespace wsb {
 // ---------------------------------------------------------------------------
 constexpr int kThreads = 256;        // threads per CTA for every solver kernel
 constexpr int kTileRows = 256;       // rows (or block rows x 6) per tile, <= kThreads
-constexpr int kCsrCap = 6144;        // CSR nonzeros per SpMV tile (one TMA stage)
-constexpr int kBsrCapBlocks = 256;   // BSR 6x6 blocks per SpMV tile (36 KiB of values)
+constexpr int kCsrCap = 4096;        // CSR nonzeros per SpMV tile (one TMA stage)
+constexpr int kBsrCapBlocks = 192;   // BSR 6x6 blocks per SpMV tile (27 KiB of values)
 constexpr int kUpdBlocks = 64;       // block-Jacobi blocks per update tile
 constexpr int kChunkRows = 4096;     // rows per work item of the vector kernels
 constexpr int kPadElems = 64;        // tail padding of streamed arrays (elements)
