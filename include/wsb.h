@@ -139,6 +139,20 @@ int wsb_pcg_update_scalars(wsb_context *ctx, wsb_buffer *scalar_results, uint32_
                            uint32_t rz_new_index, uint32_t rz_old_index, uint32_t alpha_index,
                            uint32_t minus_alpha_index, uint32_t beta_index);
 
+/* Allocation-free dot product. No counterpart in the reference: it is the
+ * dot pass structure above (256-wide FP32 tree, result identical to
+ * wsb_dot_scalar_executor_dot_into) for callers that cannot allocate device
+ * memory where they need it (a spent memory budget, no tolerance for the
+ * synchronisation cudaMalloc can cause). d_a, d_b: n floats and d_out: one
+ * float, all device memory owned by the caller. Scratch between passes is a
+ * static device array of this library (held by every GPU that loads it until
+ * exit), which limits n to WSB_NOALLOC_DOT_MAX_N; larger n returns
+ * WSB_ERR_BAD_INPUT. The first call on a device resolves that array's
+ * address; make it before any stream capture. Calls that overlap on the GPU
+ * share the array and race. Enqueued on the context's stream; not waited for. */
+#define WSB_NOALLOC_DOT_MAX_N 16777216u
+int wsb_dot_tree256_noalloc(wsb_context *ctx, const float *d_a, const float *d_b, uint32_t n, float *d_out);
+
 /* ------------------------------------------------------------------------- */
 /* Host-side block-Jacobi setup (no GPU needed)                              */
 /* ------------------------------------------------------------------------- */

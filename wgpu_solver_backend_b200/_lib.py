@@ -93,6 +93,7 @@ SIGNATURES = {
     "wsb_block_jacobi_executor_apply": (C.c_int, [vp, vp, vp]),
     "wsb_block_jacobi_executor_destroy": (None, [vp]),
     "wsb_pcg_update_scalars": (C.c_int, [vp, vp] + [C.c_uint32] * 6),
+    "wsb_dot_tree256_noalloc": (C.c_int, [vp, vp, vp, C.c_uint32, vp]),
     "wsb_lu_factor_inplace_6": (C.c_int, [f32p, C.c_uint64, C.c_uint32]),
     "wsb_build_lu_blocks_from_csr_block_starts_6": (C.c_int, [C.c_uint32, u32p, C.c_uint64, u32p, C.c_uint64, f32p,
                                                               C.c_uint64, u32p, C.c_uint64, f32p]),
