@@ -118,12 +118,35 @@ def barrier(world):
 
 
 # ---------------------------------------------------------------------------
+# serve: the request set
+# ---------------------------------------------------------------------------
+SERVE = dict(requests=64, side_min=4, side_max=64, aniso=2.0, target=1e-8, inner=1e-4, max_iter=60000, seed=7)
+
+
+def serve_requests(n_req=None, seed=None):
+    """(side, seed) per request: lattice side log-uniform on [4, 64], each
+    system with its own seed (anisotropy 10^U(-2,2) per edge)."""
+    n_req = SERVE["requests"] if n_req is None else n_req
+    seed = SERVE["seed"] if seed is None else seed
+    rng = np.random.default_rng(seed)
+    u = rng.uniform(np.log(SERVE["side_min"]), np.log(SERVE["side_max"] + 1), n_req)
+    sides = np.clip(np.floor(np.exp(u)).astype(int), SERVE["side_min"], SERVE["side_max"])
+    return [(int(sd), 7_000_000 + 1000 * seed + i) for i, sd in enumerate(sides)]
+
+
+def serve_system(side, seed):
+    import wgpu_solver_backend_b200 as wsb
+
+    return wsb.lattice_generate(side, seed=seed, aniso_log10=SERVE["aniso"])
+
+
+# ---------------------------------------------------------------------------
 # plain80
 # ---------------------------------------------------------------------------
 PLAIN = dict(side=80, seed=2024, rel_tol=1e-6, max_iter=20000)
 
 
-def cpu_baseline_plain(sysm, lu, gpu_iters, sample_iters=8):
+def cpu_baseline_plain(sysm, lu, gpu_iters, sample_iters=600):
     """Times the oracle's FP32 restatement (all host threads) on a bounded
     sample of PCG iterations of the same system and scales to one solve."""
     import oracle
@@ -236,7 +259,7 @@ def run_reference_plain(args, world, rank, local):
     full_iters = int(os.environ.get("WSB_PLAIN80_ITERS", "0")) or 1000
     per = []
     for _ in range(args.warmup + args.steps):
-        cb = cpu_baseline_plain(s, lu, full_iters, sample_iters=4)
+        cb = cpu_baseline_plain(s, lu, full_iters, sample_iters=100)
         per.append(cb)
     vals = [c["value"] for c in per[args.warmup:]]
     v = float(np.mean(vals))
@@ -246,6 +269,235 @@ def run_reference_plain(args, world, rank, local):
             "config": {"workload": "plain80: one 80^3-node lattice system, n=3072000, nnz=127641600, tol 1e-6"},
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": per[-1]["cores"], "kind": "port",
                              "sample": per[-1]["sample"]},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def mixed_kw():
+    import wgpu_solver_backend_b200 as wsb
+
+    return dict(max_iter=SERVE["max_iter"], rel_tol=0.0, precision=wsb.PREC_MIXED_F64_IR,
+                target_relres=SERVE["target"], inner_rel_tol=SERVE["inner"])
+
+
+def served_pass(srv, pool, arrivals=None):
+    """Submits every request (at its arrival time, or all at once), waits for
+    all. Returns (makespan_s, latencies_ms, results)."""
+    kw = mixed_kw()
+    t0 = time.perf_counter()
+    rids = []
+    for i, s in enumerate(pool):
+        if arrivals is not None:
+            dt = t0 + arrivals[i] - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+        rids.append(srv.submit(s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], s["b"], **kw))
+    res = [srv.wait(r, 600.0) for r in rids]
+    mk = time.perf_counter() - t0
+    return mk, [r[1]["total_ms"] for r in res], [r[1] for r in res]
+
+
+def cpu_baseline_serve(pool, sample_iters=200):
+    """The oracle's FP32 restatement of the reference solve (all host threads)
+    timed for a few PCG iterations on every request of the set, scaled by the
+    reference algorithm's own iteration count for that request at relative
+    tolerance 1e-8 (oracle/serve_reference_iterations.json)."""
+    import oracle
+
+    import wgpu_solver_backend_b200 as wsb
+
+    path = os.path.join(ROOT, "oracle", "serve_reference_iterations.json")
+    if not os.path.exists(path):
+        return {"value": None, "unit": "solves/s", "cores": oracle.num_threads(), "kind": "port",
+                "sample": "unavailable: oracle/serve_reference_iterations.json missing"}
+    with open(path) as f:
+        ref = {(r["side"], r["seed"]): r for r in json.load(f)["requests"]}
+    total_s, measured_s, iters_total = 0.0, 0.0, 0
+    for s in pool:
+        key = (s["side"], s["seed"])
+        n = s["n"]
+        lu = wsb.build_lu_blocks_from_csr_block_starts_6(n, s["row_ptr"], s["col_idx"], s["values"],
+                                                         s["block_starts"])
+        t0 = time.perf_counter()
+        r = oracle.pcg_ref_f32(s["row_ptr"], s["col_idx"], s["values"], lu, s["block_starts"], s["b"],
+                               np.zeros(n, np.float32), sample_iters, SERVE["target"], 0.0)
+        dt = time.perf_counter() - t0
+        measured_s += dt
+        it = ref[key]["iterations"]
+        iters_total += it
+        total_s += dt / max(1, r["iterations"]) * it
+    return {"value": len(pool) / total_s, "unit": "solves/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"{sample_iters} oracle FP32 PCG iterations on each of the {len(pool)} requests "
+                      f"({measured_s:.1f} s, {oracle.num_threads()} threads), scaled by the reference "
+                      f"algorithm's iteration count per request at rel 1e-8 ({iters_total} in all)"}
+
+
+def run_serve(args, world, rank, local):
+    import torch
+
+    import wgpu_solver_backend_b200 as wsb
+
+    torch.cuda.set_device(local)
+    ctx = wsb.GpuContext.create("auto", local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    reqs = serve_requests()
+    t_gen = time.perf_counter()
+    pool = []
+    for side, seed in reqs:
+        sysm = serve_system(side, seed)
+        sysm["side"], sysm["seed"] = side, seed
+        pool.append(sysm)
+    t_gen = time.perf_counter() - t_gen
+    R = len(pool)
+    n_total = sum(p["n"] for p in pool)
+    kw = mixed_kw()
+    srv = wsb.Server(ctx, memory_budget_bytes=120 << 30, iters_per_step=16)
+    for _ in range(args.warmup):
+        served_pass(srv, pool[: min(8, R)])
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    mks, lats, results = [], [], []
+    for _ in range(args.steps):
+        mk, lat, res = served_pass(srv, pool)
+        mks.append(mk)
+        lats += lat
+        results += res
+    clk = clocks.stop()
+    e2e_s = reduce_max(sum(mks), world)
+    ok = sum(1 for r in results if r["rc"] == 0)
+    failures = [{"path": "server", "side": pool[i % R]["side"], "seed": pool[i % R]["seed"], "rc": r["rc"],
+                 "iterations": r["iterations"], "sweeps": r["refine_sweeps"], "relres": r["final_relres"],
+                 "breakdown": r["breakdown_kind"]} for i, r in enumerate(results) if r["rc"] != 0]
+    relres_max = max(r["final_relres"] for r in results)
+    iters = [r["iterations"] for r in results[:R]]
+    # Latency under open-loop Poisson arrivals at 70% of the measured capacity.
+    lam = 0.7 * R / (sum(mks) / len(mks))
+    rng = np.random.default_rng(11)
+    arrivals = np.cumsum(rng.exponential(1.0 / lam, R)) - 0.0
+    mk_p, lat_p, _ = served_pass(srv, pool, arrivals)
+    st = srv.stats()
+    srv.close()
+    # Resident batch: matrices already in HBM, one batched solve of the set.
+    mats = [wsb.Matrix.create(ctx, p["row_ptr"], p["col_idx"], p["values"], p["block_starts"]) for p in pool]
+    dev_s, batch_launches = 0.0, 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(args.steps):
+        bt = wsb.Batch(ctx)
+        for m, p in zip(mats, pool):
+            bt.add(m, p["b"], **kw)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        bt.solve()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dev_s += e0.elapsed_time(e1) / 1e3
+        for i, p in enumerate(pool):
+            _, r = bt.result(i, p["n"])
+            if i == 0:
+                batch_launches += r["kernel_launches"]
+            if r["rc"] != 0:
+                failures.append({"path": "batch", "side": p["side"], "seed": p["seed"], "rc": r["rc"],
+                                 "iterations": r["iterations"], "sweeps": r["refine_sweeps"],
+                                 "relres": r["final_relres"], "breakdown": r["breakdown_kind"]})
+        del bt
+    dev_s = reduce_max(dev_s, world)
+    # Plain baseline: the same requests one at a time (host arrays, matrix
+    # upload and LU per request, then the solve), as a plain per-solve GPU PCG.
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain_lat = []
+    for p in pool:
+        t1 = time.perf_counter()
+        m = wsb.Matrix.create(ctx, p["row_ptr"], p["col_idx"], p["values"], p["block_starts"])
+        _, r = m.solve(p["b"], raise_on_error=False, **kw)
+        if r["rc"] != 0:
+            failures.append({"path": "plain", "side": p["side"], "seed": p["seed"], "rc": r["rc"],
+                             "iterations": r["iterations"], "sweeps": r["refine_sweeps"],
+                             "relres": r["final_relres"], "breakdown": r["breakdown_kind"]})
+        del m
+        plain_lat.append((time.perf_counter() - t1) * 1e3)
+    plain_s = time.perf_counter() - t0
+    # Plain resident: the matrices already in HBM, solved one after another.
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for m, p in zip(mats, pool):
+        m.solve(p["b"], raise_on_error=False, **kw)
+    torch.cuda.synchronize()
+    plain_res_s = time.perf_counter() - t0
+    # Dominant kernel (SpMV + p.Ap) on the largest system of the set.
+    big = int(np.argmax([p["n"] for p in pool]))
+    d_b = torch.from_numpy(pool[big]["b"]).cuda()
+    torch.cuda.synchronize()
+    kt = mats[big].kernel_times(d_b.data_ptr(), iterations=10)
+    info = mats[big].info
+    peak, peak_kind = peaks()
+    spmv_gbs = info["spmv_bytes"] / (kt["spmv_ms"] / 1e3) / 1e9
+    upd_bytes = 28 * pool[big]["n"] + 144 * info["num_blocks"]
+    e2e = world * args.steps * R / e2e_s
+    line = {
+        "metric": METRIC, "value": world * args.steps * R / dev_s, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 reductions + f64 refinement)",
+        "data": "synthetic 6-DOF lattice systems, seeded",
+        "config": {"workload": f"serve: {R} requests, lattice side log-uniform [4,64] (n 384..1,572,864, "
+                               f"{n_total} unknowns in all), anisotropy 10^U(-2,2), true FP64 relres 1e-8 "
+                               f"by FP64 refinement around FP32 PCG",
+                   "step": "one pass over the request set", "value_path": "resident batch (wsb_batch)",
+                   "e2e_path": "continuous-batching server (wsb_server, host arrays)",
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (%.1f GB of matrices)"
+                   % (sum(m.info["device_bytes"] for m in mats) / 1e9)},
+        "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": int(sum(
+            4 * (len(p["row_ptr"]) + len(p["col_idx"]) + len(p["values"]) + len(p["block_starts"]) + 2 * p["n"])
+            for p in pool)), "d2h_bytes_per_step": int(sum(4 * p["n"] for p in pool))},
+        "latency_ms": {"p50": float(np.percentile(lat_p, 50)), "p99": float(np.percentile(lat_p, 99)),
+                       "arrival_rate_per_s": lam, "burst_p50": float(np.percentile(lats, 50)),
+                       "burst_p99": float(np.percentile(lats, 99))},
+        "plain_sequential": {"solves_per_s": R / plain_s, "resident_solves_per_s": R / plain_res_s,
+                             "p50_ms": float(np.percentile(plain_lat, 50)), "p99_ms": float(np.percentile(plain_lat, 99))},
+        "speedup_vs_plain": {"e2e": e2e / (world * R / plain_s), "resident": (world * args.steps * R / dev_s) /
+                             (world * R / plain_res_s)},
+        "results": {"ok": ok, "of": len(results), "max_final_relres": relres_max,
+                    "iterations_min_median_max": [int(min(iters)), int(np.median(iters)), int(max(iters))]},
+        "roofline": {"bound": "hbm", "kernel": "k_spmv_loop (SpMV + p.Ap), largest system of the set",
+                     "achieved": spmv_gbs, "peak": peak, "unit": "GB/s", "frac": spmv_gbs / peak,
+                     "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": info["spmv_bytes"],
+                     "launch_us": kt["spmv_ms"] * 1e3,
+                     "update_kernel_gbs": upd_bytes / kt["update_ms"] / 1e6},
+        "server": {"steps": st["steps"], "device_bytes_peak": st["device_bytes_peak"]},
+        "failures": failures[:20],
+        "host_generate_s": t_gen,
+        "gpu_launches": batch_launches,
+        "server_kernel_launches_all_passes": st["kernel_launches"],
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_baseline_serve(pool)
+    return line
+
+
+def run_reference_serve(args, world, rank, local):
+    reqs = serve_requests()
+    pool = []
+    for side, seed in reqs:
+        sysm = serve_system(side, seed)
+        sysm["side"], sysm["seed"] = side, seed
+        pool.append(sysm)
+    vals = []
+    for k in range(args.warmup + args.steps):
+        cb = cpu_baseline_serve(pool, sample_iters=60)
+        if k >= args.warmup:
+            vals.append(cb["value"])
+    v = float(np.mean(vals))
+    return {"metric": METRIC, "impl": "reference", "value": v, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": len(pool) / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic 6-DOF lattice systems, seeded",
+            "config": {"workload": f"serve: {len(pool)} requests, lattice side log-uniform [4,64], anisotropy "
+                                   f"10^U(-2,2), relres 1e-8 (the reference's FP32 recursive residual)"},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cb["cores"], "kind": "port",
+                             "sample": cb["sample"]},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -281,10 +533,10 @@ def run_kernels(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="plain80", choices=["plain80", "kernels"])
+    ap.add_argument("--workload", default="serve", choices=["serve", "plain80", "kernels"])
     ap.add_argument("--side", type=int, default=56, help="kernels workload: lattice side")
     ap.add_argument("--iters", type=int, default=5, help="kernels workload: timed iterations")
     ap.add_argument("--layout", default="auto", choices=["auto", "csr"])
@@ -297,7 +549,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        line = run_reference_plain(args, world, rank, local)
+        line = (run_reference_serve if args.workload == "serve" else run_reference_plain)(args, world, rank, local)
         print(json.dumps(line), flush=True)
         return
     if world > 1:
@@ -308,7 +560,7 @@ def main():
 
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    line = run_plain(args, world, rank, local)
+    line = (run_serve if args.workload == "serve" else run_plain)(args, world, rank, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -214,6 +214,7 @@ typedef struct wsb_solve_result {
     double device_ms;            /* device time of the solve (CUDA events), excludes host copies */
     double total_ms;             /* host wall time of the call */
     uint64_t history_len;        /* entries written to history_out */
+    uint64_t kernel_launches;    /* kernels this library launched for the solve (0 for REFERENCE_F32) */
 } wsb_solve_result;
 
 /* ------------------------------------------------------------------------- */
@@ -301,6 +302,7 @@ typedef struct wsb_server_stats {
     uint64_t steps;
     uint64_t device_bytes_in_use, device_bytes_peak;
     double busy_ms;
+    uint64_t kernel_launches;   /* kernels the scheduler has launched so far */
 } wsb_server_stats;
 
 int wsb_server_create(wsb_context *ctx, const wsb_server_opts *opts, wsb_server **out);

@@ -38,7 +38,7 @@ class SolveResult(C.Structure):
     _fields_ = [("status", C.c_int32), ("breakdown_kind", C.c_int32), ("iterations", C.c_uint64),
                 ("refine_sweeps", C.c_uint32), ("reserved", C.c_uint32), ("b_norm2", C.c_double),
                 ("final_r_norm2", C.c_double), ("final_relres", C.c_double), ("device_ms", C.c_double),
-                ("total_ms", C.c_double), ("history_len", C.c_uint64)]
+                ("total_ms", C.c_double), ("history_len", C.c_uint64), ("kernel_launches", C.c_uint64)]
 
 
 class MatrixInfo(C.Structure):
@@ -55,7 +55,8 @@ class ServerOpts(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
                 ("rejected", C.c_uint64), ("active", C.c_uint64), ("pending", C.c_uint64), ("steps", C.c_uint64),
-                ("device_bytes_in_use", C.c_uint64), ("device_bytes_peak", C.c_uint64), ("busy_ms", C.c_double)]
+                ("device_bytes_in_use", C.c_uint64), ("device_bytes_peak", C.c_uint64), ("busy_ms", C.c_double),
+                ("kernel_launches", C.c_uint64)]
 
 
 class LatticeSizes(C.Structure):

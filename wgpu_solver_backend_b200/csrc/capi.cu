@@ -31,7 +31,7 @@ int fail(Context *ctx, int status, const char *f, ...) {
     return status;
 }
 
-int dev_alloc(Context *ctx, void **p, size_t bytes, bool zero) {
+int dev_alloc(Context *ctx, void **p, size_t bytes, bool zero, cudaStream_t stream) {
     *p = nullptr;
     if (bytes == 0) bytes = 16;
     cudaError_t e = cudaMalloc(p, bytes);
@@ -41,8 +41,8 @@ int dev_alloc(Context *ctx, void **p, size_t bytes, bool zero) {
                     "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
     }
     if (zero) {
-        e = cudaMemset(*p, 0, bytes);
-        if (e != cudaSuccess) return fail(ctx, WSB_ERR_CUDA, "cudaMemset failed: %s", cudaGetErrorString(e));
+        e = cudaMemsetAsync(*p, 0, bytes, stream);
+        if (e != cudaSuccess) return fail(ctx, WSB_ERR_CUDA, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
     }
     return WSB_OK;
 }
@@ -84,7 +84,7 @@ static int solve_reference(Context *ctx, const MatA &A, const Precond &M, const 
                          (hist_cap + 1) * sizeof(double);
     static_assert(sizeof(RefState) <= 256, "RefState fits its slot");
     void *mem = nullptr;
-    int rc = dev_alloc(ctx, &mem, total, true);  // zero: wgpu buffers start zeroed
+    int rc = dev_alloc(ctx, &mem, total, true, st);  // zero: wgpu buffers start zeroed
     if (rc) return rc;
     std::unique_ptr<void, void (*)(void *)> guard(mem, dev_free);
     char *p = static_cast<char *>(mem);
@@ -331,18 +331,18 @@ extern "C" int wsb_buffer_create(wsb_context *ctx, const void *data, size_t byte
     auto *b = new wsb_buffer();
     b->ctx = ctx;
     b->bytes = bytes;
-    int rc = dev_alloc(ctx, &b->ptr, bytes + 64, true);
+    int rc = dev_alloc(ctx, &b->ptr, bytes + 64, true, ctx->stream);
     if (rc) {
         delete b;
         return rc;
     }
-    if (data && bytes) {
-        cudaError_t e = cudaMemcpy(b->ptr, data, bytes, cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) {
-            dev_free(b->ptr);
-            delete b;
-            return fail(ctx, WSB_ERR_CUDA, "buffer upload failed: %s", cudaGetErrorString(e));
-        }
+    cudaError_t e = cudaSuccess;
+    if (data && bytes) e = cudaMemcpyAsync(b->ptr, data, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        dev_free(b->ptr);
+        delete b;
+        return fail(ctx, WSB_ERR_CUDA, "buffer upload failed: %s", cudaGetErrorString(e));
     }
     *out = b;
     return WSB_OK;
@@ -434,7 +434,7 @@ extern "C" int wsb_dot_scalar_executor_create(wsb_context *ctx, uint64_t n_max, 
     int rc = wsb_buffer_create(ctx, nullptr, std::max<size_t>(len, 1) * sizeof(float), &ex->scalars);
     if (!rc) {
         void *p = nullptr;
-        rc = dev_alloc(ctx, &p, ref_dot_scratch_floats(n_max) * sizeof(float), true);
+        rc = dev_alloc(ctx, &p, ref_dot_scratch_floats(n_max) * sizeof(float), true, ctx->stream);
         ex->scratch = static_cast<float *>(p);
     }
     if (rc) {
@@ -617,6 +617,7 @@ static int engine_solve(Context *ctx, std::unique_ptr<Engine> *eng, uint32_t *sl
         *slot_cfg = cfg;
     }
     Engine &E = **eng;
+    const uint64_t launches0 = E.launches();
     if ((rc = E.set_rhs(*slot, b, x, dev))) return rc;
     if ((rc = E.run())) return rc;
     SolveOutcome out;
@@ -637,6 +638,7 @@ static int engine_solve(Context *ctx, std::unique_ptr<Engine> *eng, uint32_t *sl
         res->device_ms = E.last_device_ms();
         res->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         res->history_len = hl;
+        res->kernel_launches = E.launches() - launches0;
     }
     return solve_status_message(ctx, out.status, out.breakdown, cfg.max_iter);
 }
@@ -809,7 +811,7 @@ extern "C" int wsb_matrix_spmv_device(wsb_context *ctx, wsb_matrix *m, const flo
     if (!sc.dd || sc.dev != ctx->device) {
         WSB_CUDA_TRY(ctx, cudaMalloc(&sc.dd, sizeof(SysDesc)));
         WSB_CUDA_TRY(ctx, cudaMalloc(&sc.sp, sizeof(StepParams)));
-        WSB_CUDA_TRY(ctx, cudaMemset(sc.sp, 0, sizeof(StepParams)));
+        WSB_CUDA_TRY(ctx, cudaMemsetAsync(sc.sp, 0, sizeof(StepParams), ctx->stream));
         sc.dev = ctx->device;
         cudaFuncSetAttribute(k_spmv_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpmvSmem);
     }
@@ -927,6 +929,7 @@ extern "C" int wsb_batch_result(wsb_batch *bt, uint32_t id, float *x, wsb_solve_
         res->final_relres = out.relres;
         res->device_ms = bt->device_ms;
         res->history_len = hl;
+        res->kernel_launches = bt->eng->launches();
     }
     return solve_status_message(ctx, out.status, out.breakdown, it.cfg.max_iter);
 }

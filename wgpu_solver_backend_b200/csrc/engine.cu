@@ -32,7 +32,7 @@ template <class T>
 static int upload(Context *ctx, T **dst, const T *src, size_t count, size_t pad, cudaStream_t st, uint64_t *bytes) {
     void *p = nullptr;
     const size_t nbytes = (count + pad) * sizeof(T);
-    int rc = dev_alloc(ctx, &p, nbytes, pad > 0);
+    int rc = dev_alloc(ctx, &p, nbytes, pad > 0, st);
     if (rc) return rc;
     *dst = static_cast<T *>(p);
     if (count) WSB_CUDA_TRY(ctx, cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, st));
@@ -152,7 +152,7 @@ Engine::Engine(Context *ctx, cudaStream_t stream) : ctx_(ctx), stream_(stream) {
     std::memset(h_sp_, 0, sizeof(StepParams));
     std::memset(h_sp_rb_, 0, sizeof(StepParams));
     cudaMalloc(&d_sp_, sizeof(StepParams));
-    cudaMemset(d_sp_, 0, sizeof(StepParams));
+    cudaMemsetAsync(d_sp_, 0, sizeof(StepParams), stream_);
 }
 
 Engine::~Engine() {
@@ -186,16 +186,17 @@ int Engine::ensure_capacity(uint32_t need) {
     WSB_CUDA_TRY(ctx_, cudaMallocHost(&hst, sizeof(SysState) * nc));
     std::memset(hs, 0, sizeof(SysDesc) * nc);
     std::memset(hst, 0, sizeof(SysState) * nc);
-    WSB_CUDA_TRY(ctx_, cudaMemset(ds, 0, sizeof(SysDesc) * nc));
-    WSB_CUDA_TRY(ctx_, cudaMemset(dst, 0, sizeof(SysState) * nc));
+    WSB_CUDA_TRY(ctx_, cudaMemsetAsync(ds, 0, sizeof(SysDesc) * nc, stream_));
+    WSB_CUDA_TRY(ctx_, cudaMemsetAsync(dst, 0, sizeof(SysState) * nc, stream_));
     if (cap_) {
         std::memcpy(hs, h_sys_, sizeof(SysDesc) * cap_);
-        WSB_CUDA_TRY(ctx_, cudaMemcpy(dst, d_state_, sizeof(SysState) * cap_, cudaMemcpyDeviceToDevice));
+        WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(dst, d_state_, sizeof(SysState) * cap_, cudaMemcpyDeviceToDevice, stream_));
         std::memcpy(hst, h_state_, sizeof(SysState) * cap_);
     }
     // Re-point every slot's state pointer at the new state array.
     for (uint32_t i = 0; i < cap_; ++i) hs[i].st = dst + i;
-    if (cap_) WSB_CUDA_TRY(ctx_, cudaMemcpy(ds, hs, sizeof(SysDesc) * cap_, cudaMemcpyHostToDevice));
+    if (cap_) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(ds, hs, sizeof(SysDesc) * cap_, cudaMemcpyHostToDevice, stream_));
+    WSB_CUDA_TRY(ctx_, cudaStreamSynchronize(stream_));
     cudaFree(d_sys_);
     cudaFree(d_state_);
     cudaFreeHost(h_sys_);
@@ -492,6 +493,7 @@ int Engine::launch_aux(const std::vector<uint32_t> &ids, int which) {
     else if (which == AUX_RESID) k_resid64<<<g, kThreads, 0, stream_>>>(d_sys_, d_sp_);
     else k_x64_to_x32<<<g, kThreads, 0, stream_>>>(d_sys_, d_sp_);
     WSB_CUDA_TRY(ctx_, cudaGetLastError());
+    launches_ += 1;
     return WSB_OK;
 }
 
@@ -694,7 +696,9 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
     (void)body_iters;
     WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(h_sp_rb_, d_sp_, sizeof(StepParams), cudaMemcpyDeviceToHost, stream_));
     WSB_CUDA_TRY(ctx_, cudaStreamSynchronize(stream_));
-    if (num_active_ > 0 && n_work_a_ > 0) launches_ += 1 + 3ull * h_sp_rb_->loop_count;
+    // Graph: the gate kernel once, then three body kernels per loop pass.
+    if (num_active_ > 0 && n_work_a_ > 0)
+        launches_ += use_graph_ ? 1 + 3ull * h_sp_rb_->loop_count : 3ull * h_sp_->loop_count;
     if (h_sp_rb_->error) {
         // A bounded wait ran out inside a kernel: end every system in flight.
         const uint32_t code = h_sp_rb_->error;

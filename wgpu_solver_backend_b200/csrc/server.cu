@@ -11,6 +11,7 @@
 //    then retires finished systems (x copied out, memory released).
 // A request that cannot fit the budget even alone is rejected with
 // WSB_ERR_OUT_OF_MEMORY; others wait until enough memory is released.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -66,7 +67,8 @@ uint64_t estimate_bytes(const Request &r) {
 struct wsb_server {
     Context *ctx = nullptr;
     wsb_server_opts opts{};
-    cudaStream_t stream = nullptr, upload_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::vector<cudaStream_t> upload_streams;
     std::unique_ptr<Engine> eng;
     std::mutex mu;
     std::condition_variable cv_upload, cv_sched, cv_done;
@@ -78,7 +80,8 @@ struct wsb_server {
     uint64_t bytes_in_use = 0, bytes_peak = 0;
     wsb_server_stats stats{};
     bool stopping = false;
-    std::thread uploader, scheduler;
+    std::vector<std::thread> uploaders;
+    std::thread scheduler;
     std::string fatal;
 
     void finish(Request *r, int status, const std::string &err) {
@@ -98,7 +101,7 @@ struct wsb_server {
         else ++stats.failed;
     }
 
-    void upload_loop() {
+    void upload_loop(cudaStream_t upload_stream) {
         cudaSetDevice(ctx->device);
         for (;;) {
             Request *r = nullptr;
@@ -195,6 +198,7 @@ struct wsb_server {
             std::lock_guard<std::mutex> lk(mu);
             stats.steps += 1;
             stats.busy_ms += ms;
+            stats.kernel_launches = eng->launches();
             if (rc) {
                 // A device error ends every active request.
                 fatal = thread_error();
@@ -247,13 +251,20 @@ extern "C" int wsb_server_create(wsb_context *ctx_in, const wsb_server_opts *opt
     if (s->opts.memory_budget_bytes == 0) s->opts.memory_budget_bytes = 120ull << 30;
     if (s->opts.iters_per_step == 0) s->opts.iters_per_step = 16;
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->upload_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete s;
         return fail(ctx, WSB_ERR_CUDA, "server stream creation failed: %s", cudaGetErrorString(e));
     }
     s->eng.reset(new Engine(ctx, s->stream));
-    s->uploader = std::thread([s] { s->upload_loop(); });
+    // Several uploaders: host preparation of one large request (validation,
+    // LU, BSR6 conversion, copies) overlaps with that of the next ones.
+    const unsigned n_up = std::max(1u, std::min(4u, std::thread::hardware_concurrency() / 2));
+    for (unsigned i = 0; i < n_up; ++i) {
+        cudaStream_t us = nullptr;
+        if (cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking) != cudaSuccess) break;
+        s->upload_streams.push_back(us);
+    }
+    for (cudaStream_t us : s->upload_streams) s->uploaders.emplace_back([s, us] { s->upload_loop(us); });
     s->scheduler = std::thread([s] { s->sched_loop(); });
     *out = s;
     return WSB_OK;
@@ -366,12 +377,13 @@ extern "C" void wsb_server_destroy(wsb_server *s) {
     }
     s->cv_upload.notify_all();
     s->cv_sched.notify_all();
-    if (s->uploader.joinable()) s->uploader.join();
+    for (auto &t : s->uploaders)
+        if (t.joinable()) t.join();
     if (s->scheduler.joinable()) s->scheduler.join();
     cudaSetDevice(s->ctx->device);
     s->eng.reset();
     s->table.clear();
     cudaStreamDestroy(s->stream);
-    cudaStreamDestroy(s->upload_stream);
+    for (cudaStream_t us : s->upload_streams) cudaStreamDestroy(us);
     delete s;
 }

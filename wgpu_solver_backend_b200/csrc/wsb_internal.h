@@ -146,8 +146,11 @@ struct Buffer {
     size_t bytes = 0;
 };
 
-// Device allocation helper (zero-filled, padded).
-int dev_alloc(Context *ctx, void **p, size_t bytes, bool zero = true);
+// Device allocation; when `zero`, the zero fill is enqueued on `stream`, so
+// it is ordered before every later copy or kernel on that stream (a plain
+// cudaMemset would run on the legacy default stream, unordered with work on
+// non-blocking streams).
+int dev_alloc(Context *ctx, void **p, size_t bytes, bool zero, cudaStream_t stream);
 void dev_free(void *p);
 
 // ---------------------------------------------------------------------------
