@@ -9,6 +9,8 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
+CLI_TOOLS = ("wgpu_solver_backend_cli", "wgpu_solver_backend_convert_cli")
+BIN = os.path.join(ROOT, "wgpu_solver_backend_b200", "bin")
 
 
 def pytest_configure(config):
@@ -20,8 +22,9 @@ def _built():
     import oracle
 
     oracle.build()
-    lib = os.path.join(ROOT, "wgpu_solver_backend_b200", "libwsb.so")
-    if not os.path.exists(lib):
+    pkg = os.path.join(ROOT, "wgpu_solver_backend_b200")
+    built = [os.path.join(pkg, "libwsb.so")] + [os.path.join(pkg, "bin", t) for t in CLI_TOOLS]
+    if not all(os.path.exists(f) for f in built):
         import subprocess
 
         subprocess.check_call(["make", "-s", "-j8", "-C", os.path.join(ROOT, "wgpu_solver_backend_b200")])
