@@ -817,9 +817,9 @@ extern "C" int wsb_matrix_spmv_device(wsb_context *ctx, wsb_matrix *m, const flo
     }
     WSB_CUDA_TRY(ctx, cudaMemcpyAsync(sc.dd, &d, sizeof d, cudaMemcpyHostToDevice, ctx->stream));
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_spmv_plain, kPipeThreads, kSpmvSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_spmv_plain, kSpmvThreads, kSpmvSmem);
     const uint32_t g = std::max<uint32_t>(1, std::min<uint32_t>(m->A.n_stiles, (uint32_t)(std::max(occ, 1) * ctx->sm_count)));
-    k_spmv_plain<<<g, kPipeThreads, kSpmvSmem, ctx->stream>>>(sc.dd, sc.sp, d_x, d_y);
+    k_spmv_plain<<<g, kSpmvThreads, kSpmvSmem, ctx->stream>>>(sc.dd, sc.sp, d_x, d_y);
     WSB_CUDA_TRY(ctx, cudaGetLastError());
     return WSB_OK;
 }

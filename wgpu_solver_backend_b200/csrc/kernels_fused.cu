@@ -55,6 +55,42 @@ __device__ __forceinline__ void tma_load(void *dst, const void *src, uint32_t by
                  : "memory");
 }
 
+// 1-D bulk copy with an L2 evict-first hint, for data streamed once per
+// iteration (matrix values and indices, LU factors): it leaves the L2 to the
+// Krylov vectors, which the next kernels read again.
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+__device__ __forceinline__ void tma_load_stream(void *dst, const void *src, uint32_t bytes, uint64_t *bar,
+                                                uint64_t pol) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
+        : "memory");
+}
+
+// Asynchronous 4- and 8-byte copies global -> shared (cp.async): the
+// gathered x values go straight into the stage without holding registers.
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+// Arrive on an mbarrier once all of this thread's earlier cp.async copies
+// have landed (the barrier's expected count covers the arrival).
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t *bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
@@ -79,23 +115,21 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// One arrival per warp (the barrier counts warps): the warp's lanes converge
+// first, so all of their earlier shared-memory reads are done, then lane 0
+// arrives. A per-thread arrival would put 32 atomic updates of one
+// shared-memory word behind every warp.
+__device__ __forceinline__ void mbar_arrive_warp(uint64_t *bar) {
+    __syncwarp();
+    if ((threadIdx.x & 31u) == 0) mbar_arrive(bar);
+}
+
 // The pipelined kernels run kThreads consumer threads (warps 0-7) and one
-// producer warp (kPipeThreads in all); consumers synchronise among themselves
-// on named barrier 1 so the producer never has to join. Kernels without a
+// producer warp (plus a gather warp in the SpMV); consumers synchronise among
+// themselves on named barrier 1 so the other warps never have to join. Kernels without a
 // producer warp launch exactly kThreads threads and use the same barrier.
 
 __device__ __forceinline__ void csync() { asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory"); }
-
-// Consumer thread 0 waits (bounded) and shares the outcome; then every
-// consumer observes the completed phase itself (immediate), which makes the
-// TMA data and the producer's descriptor visible to it.
-__device__ __forceinline__ bool consumer_wait(uint64_t *bar, uint32_t parity, int *s_ok) {
-    if (threadIdx.x == 0) *s_ok = mbar_wait(bar, parity) ? 1 : 0;
-    csync();
-    if (!*s_ok) return false;
-    mbar_wait(bar, parity);
-    return true;
-}
 
 // ---------------------------------------------------------------------------
 // Reductions
@@ -141,6 +175,45 @@ __device__ __forceinline__ double2 block_sum2(double a, double b, double *red) {
     return make_double2(sa, sb);
 }
 
+// Sum of n FP64 partials over the consumer threads: thread t adds elements
+// t, t + kThreads, t + 2 kThreads, ... in that order (16 loads in flight),
+// then the fixed-shape block sum. Result valid in thread 0.
+__device__ __forceinline__ double sum_partials(const double *__restrict__ p, uint32_t n, double *red) {
+    double v = 0.0;
+    uint32_t i = threadIdx.x;
+    for (; i + 15u * kThreads < n; i += 16u * kThreads) {
+        double q[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) q[u] = __ldcg(p + i + u * kThreads);
+#pragma unroll
+        for (int u = 0; u < 16; ++u) v += q[u];
+    }
+    for (; i < n; i += kThreads) v += __ldcg(p + i);
+    return block_sum(v, red);
+}
+
+// The same for pairs of partials (both components in one pass).
+__device__ __forceinline__ double2 sum_partials2(const double2 *__restrict__ p, uint32_t n, double *red) {
+    double va = 0.0, vb = 0.0;
+    uint32_t i = threadIdx.x;
+    for (; i + 7u * kThreads < n; i += 8u * kThreads) {
+        double2 q[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) q[u] = __ldcg(p + i + u * kThreads);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            va += q[u].x;
+            vb += q[u].y;
+        }
+    }
+    for (; i < n; i += kThreads) {
+        const double2 q = __ldcg(p + i);
+        va += q.x;
+        vb += q.y;
+    }
+    return block_sum2(va, vb, red);
+}
+
 // Ticket on a per-system counter: this CTA adds the number of tiles whose
 // partials it has published (thread 0 wrote them); true in every thread of
 // the CTA whose tickets complete the system's total.
@@ -161,16 +234,18 @@ __device__ __forceinline__ bool take_ticket(uint32_t *counter, uint32_t cnt, uin
 // ---------------------------------------------------------------------------
 enum SpmvMode { M_LOOP = 0, M_INIT = 1, M_PLAIN = 2 };
 
-// Shared-memory stage (floats). CSR: values [0, kCsrCap+8), columns
-// [kCsrCap+8, 2(kCsrCap+8)), row pointers at kRpOff. BSR6: block values
-// [0, 36 kBsrCapBlocks), block columns at kBcolOff, row pointers at kRpOff.
+// Stage layout (floats), from kernels_fused.cuh: CSR values [0, kCsrCap+8),
+// columns at kColOff; BSR6 block values [0, 36 kBsrCapBlocks), block columns
+// at kBcolOff, gathered x at kXgOff (float2, 3 per block); row pointers at
+// kRpOff.
 constexpr int kValCap = kCsrCap + 8;
 constexpr int kColOff = kValCap;
-constexpr int kBcolOff = kBsrCapBlocks * 36;
+constexpr int kBcolOff = kSpmvBcolOff;
+constexpr int kXgOff = kSpmvXgOff;
 constexpr int kRpOff = kSpmvRpOff;
-constexpr int kXgOff = kBcolOff + kBsrCapBlocks + 8;  // BSR6: gathered x, 6 per block
-static_assert(kXgOff + 6 * kBsrCapBlocks <= kRpOff, "BSR stage fits");
-static_assert((kColOff * 4) % 16 == 0 && (kBcolOff * 4) % 16 == 0 && (kRpOff * 4) % 16 == 0, "TMA alignment");
+static_assert((kColOff * 4) % 16 == 0 && (kBcolOff * 4) % 16 == 0 && (kXgOff * 4) % 16 == 0 &&
+                  (kRpOff * 4) % 16 == 0 && (kSpmvStageFloats * 4) % 128 == 0,
+              "TMA alignment");
 static_assert(kSpmvStageFloats >= kRpOff + kTileRows + 8, "stage size");
 
 struct SpmvDesc {
@@ -182,35 +257,28 @@ struct SpmvDesc {
     uint32_t pad;
 };
 
-// Resolves the next tile of this CTA (thread 0). *w is the CTA's cursor.
+// Resolves one work index of the SpMV work list (one producer lane). False
+// for an index past the end, an invalid item (which also sets an error code)
+// and, in the loop kernel, a system that is no longer active.
 template <int kMode>
-__device__ __forceinline__ bool resolve_spmv(const SysDesc *__restrict__ sys, const StepParams *sp, uint32_t *w,
-                                             SpmvDesc *d) {
+__device__ __forceinline__ bool resolve_spmv(const SysDesc *__restrict__ sys, const StepParams *sp, uint32_t idx,
+                                             uint32_t nw, WorkItem it, SpmvDesc *d) {
+    if (idx >= nw) return false;
     if (kMode == M_PLAIN) {
-        const SysDesc &S = sys[0];
-        if (*w >= S.n_stiles) return false;
-        d->sys = 0;
-        d->tile = *w;
-        *w += gridDim.x;
+        it.sys = 0;
+        it.tile = idx;
     } else {
-        const uint32_t nw = kMode == M_INIT ? sp->n_init_a : sp->n_work_a;
-        const WorkItem *work = kMode == M_INIT ? sp->init_a : sp->work_a;
-        for (;;) {
-            if (*w >= nw) return false;
-            const WorkItem it = work[*w];
-            *w += gridDim.x;
-            if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_stiles) {
-                atomicOr(const_cast<uint32_t *>(&sp->error), 8u);  // invalid work item: skipped
-                continue;
-            }
-            if (kMode == M_LOOP && !sys[it.sys].st->active) continue;
-            d->sys = it.sys;
-            d->tile = it.tile;
-            break;
+        if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_stiles) {
+            atomicOr(const_cast<uint32_t *>(&sp->error), 8u);  // invalid work item: skipped
+            return false;
         }
+        if (kMode == M_LOOP && !sys[it.sys].st->active) return false;
     }
-    const SysDesc &S = sys[d->sys];
-    const SpmvTile T = S.stiles[d->tile];
+    const SysDesc &S = sys[it.sys];
+    const SpmvTile T = S.stiles[it.tile];
+    d->valid = 1;
+    d->sys = it.sys;
+    d->tile = it.tile;
     d->layout = S.layout;
     d->r0 = T.row0;
     d->nr = T.row1 - T.row0;
@@ -222,9 +290,9 @@ __device__ __forceinline__ bool resolve_spmv(const SysDesc *__restrict__ sys, co
     return true;
 }
 
-// Issues the bulk copies of a resolved tile into a stage (thread 0).
+// Issues the bulk copies of a resolved tile into a stage (producer lane 0).
 __device__ __forceinline__ void issue_spmv(const SysDesc *__restrict__ sys, const SpmvDesc &d, float *stage,
-                                           uint64_t *bar) {
+                                           uint64_t *bar, uint64_t pol) {
     if (d.lng) {
         mbar_expect_tx(bar, 0);
         return;
@@ -236,22 +304,43 @@ __device__ __forceinline__ void issue_spmv(const SysDesc *__restrict__ sys, cons
     if (d.layout == LAYOUT_BSR6) {
         const uint32_t vb = (d.k1 - d.k0) * 144u;
         mbar_expect_tx(bar, vb + 4u * cc + 4u * rc);
-        if (vb) tma_load(stage, S.bval + (size_t)d.k0 * 36u, vb, bar);
-        if (cc) tma_load(stage + kBcolOff, S.bcol + d.ka, 4u * cc, bar);
-        tma_load(rp, S.brow_ptr + d.ra, 4u * rc, bar);
+        if (vb) tma_load_stream(stage, S.bval + (size_t)d.k0 * 36u, vb, bar, pol);
+        if (cc) tma_load_stream(stage + kBcolOff, S.bcol + d.ka, 4u * cc, bar, pol);
+        tma_load_stream(rp, S.brow_ptr + d.ra, 4u * rc, bar, pol);
     } else {
         mbar_expect_tx(bar, 8u * cc + 4u * rc);
         if (cc) {
-            tma_load(stage, S.val + d.ka, 4u * cc, bar);
-            tma_load(stage + kColOff, S.col + d.ka, 4u * cc, bar);
+            tma_load_stream(stage, S.val + d.ka, 4u * cc, bar, pol);
+            tma_load_stream(stage + kColOff, S.col + d.ka, 4u * cc, bar, pol);
         }
-        tma_load(rp, S.row_ptr + d.ra, 4u * rc, bar);
+        tma_load_stream(rp, S.row_ptr + d.ra, 4u * rc, bar, pol);
     }
 }
 
-// CSR tile from a filled stage: products val*x[col] in place (all threads,
-// strided over the nonzeros), then one thread per row adds its products in
-// index order.
+// Gather warp, BSR6 tile in a filled stage: the 6 x values of every block
+// column into the stage's gather area as 3 float2 per block (cp.async, no
+// registers held, so the warp moves on to the next tile at once).
+__device__ __forceinline__ void gather_bsr(const SpmvDesc &d, const float *__restrict__ xin, float *stage,
+                                           uint32_t lane) {
+    const bool al8 = (reinterpret_cast<uintptr_t>(xin) & 7u) == 0;
+    const uint32_t *bcol = reinterpret_cast<const uint32_t *>(stage + kBcolOff);
+    float *xg = stage + kXgOff;
+    const uint32_t cofs = d.k0 - d.ka, ne = 3u * (d.k1 - d.k0);
+    for (uint32_t e = lane; e < ne; e += 32u) {
+        const uint32_t blk = e / 3u, h = e - 3u * blk;
+        const float *src = xin + 6u * (size_t)bcol[blk + cofs] + 2u * h;
+        if (al8) {
+            cp_async8(xg + 2u * e, src);
+        } else {  // a caller's x that is only 4-byte aligned (plain SpMV entry point)
+            cp_async4(xg + 2u * e, src);
+            cp_async4(xg + 2u * e + 1u, src + 1);
+        }
+    }
+}
+
+// CSR tile from a filled stage: products val*x[col] in place (all consumer
+// threads, strided over the nonzeros), then one thread per row adds its
+// products in index order (spmv.wgsl:58-61).
 __device__ __forceinline__ float csr_stage(const SpmvDesc &d, const float *__restrict__ xin, float *stage) {
     float *val = stage;
     const uint32_t *col = reinterpret_cast<const uint32_t *>(stage + kColOff);
@@ -276,43 +365,47 @@ __device__ __forceinline__ float csr_stage(const SpmvDesc &d, const float *__res
     return acc;
 }
 
-// BSR6 tile from a filled stage. Phase A (all threads): the 6 x values of
-// every block column are gathered into shared memory, with independent loads.
-// Phase B: thread t owns row (t/6, t%6) and walks its block row's blocks in
-// column order, six products each from shared memory, added in index order
-// (for complete 6x6 blocks with sorted columns this is the CSR order).
-__device__ __forceinline__ float bsr_stage(const SpmvDesc &d, const float *__restrict__ xin, float *stage) {
-    const uint32_t *bcol = reinterpret_cast<const uint32_t *>(stage + kBcolOff);
+// BSR6 tile from a filled and gathered stage: thread t owns row (t/6, t%6) of
+// the tile and walks its block row's blocks in column order, six products
+// each from shared memory, added in index order (for complete 6x6 blocks
+// with sorted columns this is the CSR order). With kOwn, the thread also
+// picks its own row's x value out of the diagonal block's gathered x (for
+// p.Ap without another global load); *own_ok is false when the block row
+// has no diagonal block.
+template <bool kOwn>
+__device__ __forceinline__ float bsr_stage(const SpmvDesc &d, const float *stage, float *own, bool *own_ok) {
     const uint32_t *rp = reinterpret_cast<const uint32_t *>(stage + kRpOff);
-    float *xg = stage + kXgOff;
-    const uint32_t nb = d.k1 - d.k0, cofs = d.k0 - d.ka;
-    const uint32_t ne = 6u * nb;
-    // Up to kGather independent loads per thread in flight at once.
-    constexpr int kGather = (6 * kBsrCapBlocks + kThreads - 1) / kThreads;
-    float v[kGather];
-#pragma unroll
-    for (int q = 0; q < kGather; ++q) {
-        const uint32_t e = threadIdx.x + q * kThreads;
-        v[q] = e < ne ? __ldg(xin + 6u * (size_t)bcol[e / 6u + cofs] + e % 6u) : 0.0f;
-    }
-#pragma unroll
-    for (int q = 0; q < kGather; ++q) {
-        const uint32_t e = threadIdx.x + q * kThreads;
-        if (e < ne) xg[e] = v[q];
-    }
-    csync();
-    float acc = 0.0f;
+    const uint32_t *bcol = reinterpret_cast<const uint32_t *>(stage + kBcolOff);
+    const float2 *xg = reinterpret_cast<const float2 *>(stage + kXgOff);
+    float acc = 0.0f, xo = 0.0f;
+    bool found = false;
     const uint32_t t = threadIdx.x;
     if (t < 6u * d.nr) {
         const uint32_t br = t / 6u, a = t - 6u * br;
         const uint32_t o = d.r0 - d.ra + br;
         const uint32_t s0 = rp[o] - d.k0, s1 = rp[o + 1] - d.k0;
+        const uint32_t cofs = d.k0 - d.ka, self = d.r0 + br;
         for (uint32_t blk = s0; blk < s1; ++blk) {
-            const float *B = stage + blk * 36u + a * 6u;
-            const float *X = xg + blk * 6u;
-#pragma unroll
-            for (int j = 0; j < 6; ++j) acc = __fadd_rn(acc, __fmul_rn(B[j], X[j]));
+            const float2 *B = reinterpret_cast<const float2 *>(stage + blk * 36u + a * 6u);
+            const float2 *X = xg + blk * 3u;
+            const float2 b0 = B[0], b1 = B[1], b2 = B[2];
+            const float2 x0 = X[0], x1 = X[1], x2 = X[2];
+            acc = __fadd_rn(acc, __fmul_rn(b0.x, x0.x));
+            acc = __fadd_rn(acc, __fmul_rn(b0.y, x0.y));
+            acc = __fadd_rn(acc, __fmul_rn(b1.x, x1.x));
+            acc = __fadd_rn(acc, __fmul_rn(b1.y, x1.y));
+            acc = __fadd_rn(acc, __fmul_rn(b2.x, x2.x));
+            acc = __fadd_rn(acc, __fmul_rn(b2.y, x2.y));
+            if (kOwn && bcol[blk + cofs] == self) {
+                const float2 xs = a < 2u ? x0 : (a < 4u ? x1 : x2);
+                xo = (a & 1u) ? xs.y : xs.x;
+                found = true;
+            }
         }
+    }
+    if (kOwn) {
+        *own = xo;
+        *own_ok = found;
     }
     return acc;
 }
@@ -367,9 +460,7 @@ __device__ __forceinline__ void flush_spmv(const SysDesc *__restrict__ sys, uint
     const SysDesc &S = sys[s];
     SysState *st = S.st;
     if (!take_ticket(&st->cnt_a, cnt, S.n_stiles, s_last)) return;
-    double v = 0.0;
-    for (uint32_t i = threadIdx.x; i < S.n_stiles; i += kThreads) v += __ldcg(S.part_a + i);
-    const double pap = block_sum(v, red);
+    const double pap = sum_partials(S.part_a, S.n_stiles, red);
     if (threadIdx.x == 0) {
         const double alpha = pap != 0.0 ? st->rz_old / pap : 0.0;
         st->pap = pap;
@@ -379,73 +470,184 @@ __device__ __forceinline__ void flush_spmv(const SysDesc *__restrict__ sys, uint
     }
 }
 
-// The SpMV pipeline shared by the loop, init and plain kernels. Thread
-// kThreads (lane 0 of the producer warp) resolves tiles and issues their TMA
-// copies into a two-stage ring (full barrier: copy bytes; empty barrier: one
-// arrival per consumer); the consumers compute tile after tile.
+template <int kMode>
+__device__ __forceinline__ const float *spmv_input(const SysDesc &S, const float *__restrict__ xplain) {
+    return kMode == M_PLAIN ? xplain : kMode == M_INIT ? S.x : S.p;
+}
+
+// Producer warp of the SpMV ring. The warp resolves 32 work items at once
+// (one lane each: work item -> system -> tile), so the chain of dependent
+// loads behind a tile is paid once per 32 tiles, and keeps the work items of
+// the next batch in flight meanwhile. Lane 0 then walks the batch in order:
+// it claims stage k % NS once the consumers released tile k - NS, publishes
+// the tile's descriptor and issues its bulk copies. After the last tile it
+// publishes an end marker. Every wait is bounded; on a timeout lane 0 records
+// an error, waits (bounded) for its copies still in flight and returns.
+template <int kMode>
+__device__ __forceinline__ void spmv_producer(const SysDesc *__restrict__ sys, StepParams *sp, float *smem,
+                                              uint64_t *full, uint64_t *empty, SpmvDesc *desc, SpmvDesc *bdesc) {
+    constexpr uint32_t NS = kSpmvStages;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t G = gridDim.x;
+    const uint32_t nw = kMode == M_PLAIN ? sys[0].n_stiles : kMode == M_INIT ? sp->n_init_a : sp->n_work_a;
+    const WorkItem *__restrict__ work = kMode == M_INIT ? sp->init_a : sp->work_a;
+    uint32_t base = blockIdx.x;  // work index of lane 0's item in the current batch
+    WorkItem it = {0u, 0u};
+    if (kMode != M_PLAIN && base + lane * G < nw) it = work[base + lane * G];
+    uint32_t k = 0, issued = 0;
+    bool err = false;
+    const uint64_t pol = l2_evict_first_policy();
+    for (;;) {
+        SpmvDesc d;
+        const bool ok = resolve_spmv<kMode>(sys, sp, base + lane * G, nw, it, &d);
+        const uint32_t m = __ballot_sync(0xffffffffu, ok);
+        if (ok) bdesc[__popc(m & ((1u << lane) - 1u))] = d;
+        const uint32_t cnt = __popc(m);
+        base += 32u * G;
+        const bool more = base < nw;
+        if (kMode != M_PLAIN && base + lane * G < nw) it = work[base + lane * G];  // next batch, in flight
+        __syncwarp();
+        if (lane == 0) {
+            for (uint32_t i = 0; i <= cnt; ++i) {
+                if (i == cnt && more) break;
+                const uint32_t s = k % NS;
+                if (k >= NS && !mbar_wait(&empty[s], ((k / NS) - 1) & 1u)) {
+                    atomicOr(&sp->error, 16u);
+                    err = true;
+                    break;
+                }
+                if (i < cnt) {
+                    desc[s] = bdesc[i];
+                    issue_spmv(sys, bdesc[i], smem + s * kSpmvStageFloats, &full[s], pol);
+                    issued = k + 1;
+                } else {  // end marker
+                    desc[s].valid = 0;
+                    mbar_expect_tx(&full[s], 0);
+                }
+                ++k;
+            }
+        }
+        err = __shfl_sync(0xffffffffu, err ? 1u : 0u, 0) != 0;
+        __syncwarp();  // lane 0 is done with bdesc before the next batch overwrites it
+        if (err || !more) break;
+    }
+    if (err && lane == 0) {
+        // Bounded drain of the copies that may still be in flight.
+        for (uint32_t j = issued > NS ? issued - NS : 0; j < issued; ++j) mbar_wait(&full[j % NS], (j / NS) & 1u);
+    }
+}
+
+// Gather warp of the SpMV ring: follows the tiles as they land and, for
+// BSR6 tiles, gathers the x values of every block column into the stage
+// (cp.async); the stage's gather barrier completes when those copies have
+// landed (it completes at once for tiles that need no gather). The warp never
+// waits for its own copies, so it stays ahead of the consumers.
+template <int kMode>
+__device__ __forceinline__ void spmv_gatherer(const SysDesc *__restrict__ sys, StepParams *sp,
+                                              const float *__restrict__ xplain, float *smem, uint64_t *full,
+                                              uint64_t *gath, const SpmvDesc *desc) {
+    constexpr uint32_t NS = kSpmvStages;
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t j = 0;; ++j) {
+        const uint32_t s = j % NS, par = (j / NS) & 1u;
+        uint32_t ok = 1;
+        if (lane == 0) ok = mbar_wait(&full[s], par) ? 1u : 0u;
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) {
+            if (lane == 0) atomicOr(&sp->error, 64u);
+            break;
+        }
+        mbar_wait(&full[s], par);  // completed: the stage and its descriptor are visible
+        const SpmvDesc d = desc[s];
+        if (d.valid && d.layout == LAYOUT_BSR6 && !d.lng)
+            gather_bsr(d, spmv_input<kMode>(sys[d.sys], xplain), smem + s * kSpmvStageFloats, lane);
+        cp_async_mbar_arrive(&gath[s]);
+        if (!d.valid) break;
+    }
+    cp_async_wait<0>();
+}
+
+// The SpMV pipeline shared by the loop, init and plain kernels: kThreads
+// consumer threads compute tile after tile from the ring that the producer
+// warp fills and the gather warp completes. Per tile the consumers pass one
+// barrier (the stage wait, which also separates the previous tile's warp
+// partials from their publication by thread 0).
 template <int kMode>
 __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, StepParams *sp,
                                               const float *__restrict__ xplain, float *__restrict__ yplain,
                                               float *smem) {
-    __shared__ __align__(8) uint64_t full[2], empty[2];
-    __shared__ SpmvDesc desc[2];
+    constexpr uint32_t NS = kSpmvStages;
+    __shared__ __align__(8) uint64_t full[NS], gath[NS], empty[NS];
+    __shared__ SpmvDesc desc[NS];
+    __shared__ SpmvDesc bdesc[32];
     __shared__ double red[64];
-    __shared__ int s_last, s_ok;
+    __shared__ double wred[2 * (kThreads / 32)];
+    __shared__ int s_last, s_ok[2];
     const uint32_t tid = threadIdx.x;
     if (tid == 0) {
-        mbar_init(&full[0], 1);
-        mbar_init(&full[1], 1);
-        mbar_init(&empty[0], kThreads);
-        mbar_init(&empty[1], kThreads);
+        for (uint32_t i = 0; i < NS; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&gath[i], 32);
+            mbar_init(&empty[i], kThreads / 32);
+        }
         fence_barrier_init();
     }
     __syncthreads();
     if (tid >= kThreads) {
-        if (tid != kThreads) return;
-        uint32_t w = blockIdx.x;
-        for (uint32_t k = 0;; ++k) {
-            const uint32_t s = k & 1u;
-            if (k >= 2 && !mbar_wait(&empty[s], ((k >> 1) - 1) & 1u)) {
-                atomicOr(&sp->error, 16u);
-                return;
-            }
-            SpmvDesc d;
-            d.valid = resolve_spmv<kMode>(sys, sp, &w, &d) ? 1u : 0u;
-            desc[s] = d;
-            if (d.valid) {
-                issue_spmv(sys, d, smem + s * kSpmvStageFloats, &full[s]);
-            } else {
-                mbar_expect_tx(&full[s], 0);
-                return;
-            }
-        }
+        if (tid < kThreads + 32) spmv_producer<kMode>(sys, sp, smem, full, empty, desc, bdesc);
+        else if (tid < kThreads + 64) spmv_gatherer<kMode>(sys, sp, xplain, smem, full, gath, desc);
+        return;
     }
-    uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles published since the last ticket
+    uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles of run_sys published since the last ticket
+    uint32_t pend_sys = 0, pend_tile = 0;         // thread 0: tile whose warp partials wait in wred
+    bool pend = false;
     for (uint32_t k = 0;; ++k) {
-        const uint32_t s = k & 1u;
-        if (!consumer_wait(&full[s], (k >> 1) & 1u, &s_ok)) {
-            if (tid == 0) {
-                atomicOr(&sp->error, 1u);
-                mbar_wait(&full[s ^ 1u], ((k + 1) >> 1) & 1u);  // bounded drain of the other stage
-            }
+        const uint32_t s = k % NS, par = (k / NS) & 1u;
+        // Thread 0 waits (bounded) and shares the outcome through a flag that
+        // alternates with k, so a later write never meets an earlier read.
+        if (tid == 0) s_ok[k & 1u] = (mbar_wait(&gath[s], par) && mbar_wait(&full[s], par)) ? 1 : 0;
+        csync();
+        if (!s_ok[k & 1u]) {
+            if (tid == 0) atomicOr(&sp->error, 1u);
             return;
         }
+        mbar_wait(&gath[s], par);  // completed: acquire in every thread
+        mbar_wait(&full[s], par);
         const SpmvDesc d = desc[s];
+        // The previous tile's p.Ap partial: its warps' sums in warp order.
+        if (kMode == M_LOOP && tid == 0 && pend) {
+            const double *wr = wred + 8 * ((k - 1) & 1u);
+            double v = 0.0;
+#pragma unroll
+            for (int q = 0; q < kThreads / 32; ++q) v += wr[q];
+            sys[pend_sys].part_a[pend_tile] = v;
+            pend = false;
+        }
         if (!d.valid) break;
         float *stage = smem + s * kSpmvStageFloats;
         const SysDesc &S = sys[d.sys];
-        const float *__restrict__ xin = kMode == M_PLAIN ? xplain : kMode == M_INIT ? S.x : S.p;
+        const float *__restrict__ xin = spmv_input<kMode>(S, xplain);
+        if (kMode == M_LOOP && d.sys != run_sys) {
+            flush_spmv(sys, run_sys, run_cnt, red, &s_last);
+            run_sys = d.sys;
+            run_cnt = 0;
+        }
         const uint32_t row0 = d.layout == LAYOUT_BSR6 ? 6u * d.r0 : d.r0;
         const uint32_t nrows = d.layout == LAYOUT_BSR6 ? 6u * d.nr : d.nr;
-        // p(i) of this thread's row for p.Ap, loaded ahead of the tile's work.
-        const float p_own = (kMode == M_LOOP && tid < nrows) ? __ldg(xin + row0 + tid) : 0.0f;
-        float acc;
-        if (d.lng) acc = long_tile(S, d, xin, stage);
-        else if (d.layout == LAYOUT_BSR6) acc = bsr_stage(d, xin, stage);
-        else acc = csr_stage(d, xin, stage);
-        // Everyone is done reading the stage: hand it back to the producer.
+        float acc, p_own = 0.0f;
+        bool own_ok = false;
+        if (!d.lng && d.layout == LAYOUT_BSR6) {
+            acc = bsr_stage<kMode == M_LOOP>(d, stage, &p_own, &own_ok);
+        } else {
+            if (kMode == M_LOOP && tid < nrows) {
+                p_own = __ldg(xin + row0 + tid);
+                own_ok = true;
+            }
+            acc = d.lng ? long_tile(S, d, xin, stage) : csr_stage(d, xin, stage);
+        }
+        // Done reading the stage: hand it back to the producer.
         fence_proxy_async();
-        mbar_arrive(&empty[s]);
+        mbar_arrive_warp(&empty[s]);
         if (kMode == M_PLAIN) {
             if (tid < nrows) yplain[row0 + tid] = acc;
         } else {
@@ -453,16 +655,17 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
             if (tid < nrows) {
                 const uint32_t i = row0 + tid;
                 S.ap[i] = acc;
-                if (kMode == M_LOOP) part = (double)p_own * (double)acc;
+                if (kMode == M_LOOP) {
+                    if (!own_ok) p_own = __ldg(xin + i);  // a block row without a diagonal block
+                    part = (double)p_own * (double)acc;
+                }
             }
             if (kMode == M_LOOP) {
-                const double tot = block_sum(part, red);
-                if (d.sys != run_sys) {
-                    flush_spmv(sys, run_sys, run_cnt, red, &s_last);
-                    run_sys = d.sys;
-                    run_cnt = 0;
-                }
-                if (tid == 0) S.part_a[d.tile] = tot;
+                part = warp_sum(part);
+                if ((tid & 31u) == 0) wred[8 * (k & 1u) + (tid >> 5)] = part;
+                pend = true;
+                pend_sys = d.sys;
+                pend_tile = d.tile;
                 ++run_cnt;
             }
         }
@@ -477,7 +680,7 @@ constexpr int kVecCap = kTileRows + 8;                    // floats per staged v
 constexpr int kLuOff = 4 * kVecCap;                       // LU blocks
 constexpr int kBsOff = kLuOff + kUpdBlocks * 36;          // block starts slice
 static_assert((kLuOff * 4) % 16 == 0 && (kBsOff * 4) % 16 == 0 && (kVecCap * 4) % 16 == 0, "TMA alignment");
-static_assert(kUpdStageFloats >= kBsOff + kUpdBlocks + 8, "stage size");
+static_assert(kUpdStageFloats >= kBsOff + kUpdBlocks + 8 && (kUpdStageFloats * 4) % 128 == 0, "stage size");
 
 struct UpdDesc {
     uint32_t valid, sys, tile;
@@ -487,38 +690,36 @@ struct UpdDesc {
     uint32_t pad[2];
 };
 
+// Resolves one work index of the update work list (one producer lane); false
+// past the end, for an invalid item (error code set) and, in the loop kernel,
+// for a system that is no longer active.
 template <bool kInit>
-__device__ __forceinline__ bool resolve_upd(const SysDesc *__restrict__ sys, const StepParams *sp, uint32_t *w,
-                                            UpdDesc *d) {
-    const uint32_t nw = kInit ? sp->n_init_b : sp->n_work_b;
-    const WorkItem *work = kInit ? sp->init_b : sp->work_b;
-    for (;;) {
-        if (*w >= nw) return false;
-        const WorkItem it = work[*w];
-        *w += gridDim.x;
-        if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_utiles) {
-            atomicOr(const_cast<uint32_t *>(&sp->error), 8u);  // invalid work item: skipped
-            continue;
-        }
-        if (!kInit && !sys[it.sys].st->active) continue;
-        const UpdTile T = sys[it.sys].utiles[it.tile];
-        d->sys = it.sys;
-        d->tile = it.tile;
-        d->row0 = T.row0;
-        d->rows = T.row1 - T.row0;
-        d->blk0 = T.blk0;
-        d->nblk = T.blk1 - T.blk0;
-        d->ra = T.row0 & ~3u;
-        d->ba = T.blk0 & ~3u;
-        d->alpha = kInit ? 0.0f : sys[it.sys].st->alpha_f;
-        return true;
+__device__ __forceinline__ bool resolve_upd(const SysDesc *__restrict__ sys, const StepParams *sp, uint32_t idx,
+                                            uint32_t nw, WorkItem it, UpdDesc *d) {
+    if (idx >= nw) return false;
+    if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_utiles) {
+        atomicOr(const_cast<uint32_t *>(&sp->error), 8u);  // invalid work item: skipped
+        return false;
     }
+    if (!kInit && !sys[it.sys].st->active) return false;
+    const UpdTile T = sys[it.sys].utiles[it.tile];
+    d->valid = 1;
+    d->sys = it.sys;
+    d->tile = it.tile;
+    d->row0 = T.row0;
+    d->rows = T.row1 - T.row0;
+    d->blk0 = T.blk0;
+    d->nblk = T.blk1 - T.blk0;
+    d->ra = T.row0 & ~3u;
+    d->ba = T.blk0 & ~3u;
+    d->alpha = kInit ? 0.0f : sys[it.sys].st->alpha_f;
+    return true;
 }
 
 // Stage slots: 0 = x (init: b), 1 = p, 2 = r, 3 = Ap; then LU and block starts.
 template <bool kInit>
 __device__ __forceinline__ void issue_upd(const SysDesc *__restrict__ sys, const UpdDesc &d, float *stage,
-                                          uint64_t *bar) {
+                                          uint64_t *bar, uint64_t pol) {
     const SysDesc &S = sys[d.sys];
     const uint32_t vc = ((d.row0 + d.rows - d.ra) + 3) & ~3u;
     const uint32_t bc = ((d.blk0 + d.nblk + 1 - d.ba) + 3) & ~3u;
@@ -534,21 +735,36 @@ __device__ __forceinline__ void issue_upd(const SysDesc *__restrict__ sys, const
         tma_load(stage + 2 * kVecCap, S.r + d.ra, 4u * vc, bar);
         tma_load(stage + 3 * kVecCap, S.ap + d.ra, 4u * vc, bar);
     }
-    if (lub) tma_load(stage + kLuOff, S.lu + (size_t)d.blk0 * 36u, lub, bar);
-    tma_load(stage + kBsOff, S.bstart + d.ba, 4u * bc, bar);
+    if (lub) tma_load_stream(stage + kLuOff, S.lu + (size_t)d.blk0 * 36u, lub, bar, pol);
+    tma_load_stream(stage + kBsOff, S.bstart + d.ba, 4u * bc, bar, pol);
+}
+
+// The updated residual of row o of the stage (o relative to the staged
+// range): loop r + (-alpha) Ap (axpy_from_scalar_results.wgsl), init b - A x0
+// (the reference's r = b, r += -1 * Ax).
+template <bool kInit>
+__device__ __forceinline__ float staged_r(const float *stage, uint32_t o, float ma) {
+    return kInit ? __fsub_rn(stage[o], stage[3 * kVecCap + o])
+                 : __fadd_rn(stage[2 * kVecCap + o], __fmul_rn(ma, stage[3 * kVecCap + o]));
 }
 
 // z = U^-1 L^-1 r for the blocks starting in the tile (block_jacobi.wgsl:
 // unit-L forward solve lines 93-101, U backward solve dividing by U(i,i)
 // lines 103-122, rows i < m = min(6, len) only, lines 79 and 124-126). One
-// thread per block, in registers; r from the staged slot 2.
-__device__ __forceinline__ void bj_stage(const UpdDesc &d, const float *stage, float *sz, uint32_t *sflag) {
+// thread per block, in registers. The thread forms its rows' updated r from
+// the stage itself (the same operations as the row update), so the solve
+// does not wait for the other threads. Solved rows are tagged with `tag` in
+// sflag.
+template <bool kInit>
+__device__ __forceinline__ void bj_stage(const UpdDesc &d, const float *stage, float *sz, uint32_t *sflag,
+                                         uint32_t tag) {
     const uint32_t j = threadIdx.x;
     if (j >= d.nblk) return;
     const uint32_t *bs = reinterpret_cast<const uint32_t *>(stage + kBsOff);
     const uint32_t off = bs[d.blk0 + j - d.ba], nxt = bs[d.blk0 + j + 1 - d.ba];
     const uint32_t m = min(nxt - off, 6u);
-    const float *rr = stage + 2 * kVecCap + (off - d.ra);
+    const uint32_t ro = off - d.ra;
+    const float ma = -d.alpha;
     const float *L = stage + kLuOff + j * 36u;
     const uint32_t lo = off - d.row0;
     float y[6], xs[6];
@@ -560,7 +776,7 @@ __device__ __forceinline__ void bj_stage(const UpdDesc &d, const float *stage, f
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
         if ((uint32_t)i < m) {
-            float s = rr[i];
+            float s = staged_r<kInit>(stage, ro + i, ma);
 #pragma unroll
             for (int q = 0; q < i; ++q) s = __fsub_rn(s, __fmul_rn(L[i * 6 + q], y[q]));
             y[i] = s;
@@ -580,7 +796,7 @@ __device__ __forceinline__ void bj_stage(const UpdDesc &d, const float *stage, f
     for (int i = 0; i < 6; ++i)
         if ((uint32_t)i < m) {
             sz[lo + i] = xs[i];
-            sflag[lo + i] = 1u;
+            sflag[lo + i] = tag;
         }
 }
 
@@ -598,13 +814,7 @@ __device__ __forceinline__ void flush_upd(const SysDesc *__restrict__ sys, StepP
     const SysDesc &S = sys[s];
     SysState *st = S.st;
     if (!take_ticket(&st->cnt_b, cnt, S.n_utiles, s_last)) return;
-    double va = 0.0, vb = 0.0;
-    for (uint32_t i = threadIdx.x; i < S.n_utiles; i += kThreads) {
-        const double2 q = __ldcg(S.part_b + i);
-        va += q.x;
-        vb += q.y;
-    }
-    const double2 sum = block_sum2(va, vb, red);
+    const double2 sum = sum_partials2(S.part_b, S.n_utiles, red);
     if (threadIdx.x != 0) return;
     if (kInit) {
         st->bb = sum.x;
@@ -651,109 +861,167 @@ __device__ __forceinline__ void flush_upd(const SysDesc *__restrict__ sys, StepP
     st->cnt_b = 0;
 }
 
+// Producer warp of the update ring: the same batched resolution and ring
+// discipline as the SpMV producer.
+template <bool kInit>
+__device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, StepParams *sp, float *smem,
+                                             uint64_t *full, uint64_t *empty, UpdDesc *desc, UpdDesc *bdesc) {
+    constexpr uint32_t NS = kUpdStages;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t G = gridDim.x;
+    const uint32_t nw = kInit ? sp->n_init_b : sp->n_work_b;
+    const WorkItem *__restrict__ work = kInit ? sp->init_b : sp->work_b;
+    uint32_t base = blockIdx.x;
+    WorkItem it = {0u, 0u};
+    if (base + lane * G < nw) it = work[base + lane * G];
+    uint32_t k = 0, issued = 0;
+    bool err = false;
+    const uint64_t pol = l2_evict_first_policy();
+    for (;;) {
+        UpdDesc d;
+        const bool ok = resolve_upd<kInit>(sys, sp, base + lane * G, nw, it, &d);
+        const uint32_t m = __ballot_sync(0xffffffffu, ok);
+        if (ok) bdesc[__popc(m & ((1u << lane) - 1u))] = d;
+        const uint32_t cnt = __popc(m);
+        base += 32u * G;
+        const bool more = base < nw;
+        if (base + lane * G < nw) it = work[base + lane * G];  // next batch, in flight
+        __syncwarp();
+        if (lane == 0) {
+            for (uint32_t i = 0; i <= cnt; ++i) {
+                if (i == cnt && more) break;
+                const uint32_t s = k % NS;
+                if (k >= NS && !mbar_wait(&empty[s], ((k / NS) - 1) & 1u)) {
+                    atomicOr(&sp->error, 32u);
+                    err = true;
+                    break;
+                }
+                if (i < cnt) {
+                    desc[s] = bdesc[i];
+                    issue_upd<kInit>(sys, bdesc[i], smem + s * kUpdStageFloats, &full[s], pol);
+                    issued = k + 1;
+                } else {  // end marker
+                    desc[s].valid = 0;
+                    mbar_expect_tx(&full[s], 0);
+                }
+                ++k;
+            }
+        }
+        err = __shfl_sync(0xffffffffu, err ? 1u : 0u, 0) != 0;
+        __syncwarp();
+        if (err || !more) break;
+    }
+    if (err && lane == 0) {
+        for (uint32_t j = issued > NS ? issued - NS : 0; j < issued; ++j) mbar_wait(&full[j % NS], (j / NS) & 1u);
+    }
+}
+
 // kInit = false (k_update): x += alpha p; r += (-alpha) Ap; z = M^-1 r; FP64
 // r.r and r.z per tile. kInit = true (k_init, after k_spmv_init):
 // r = b + (-1)(A x0); z = M^-1 r; p = z; FP64 b.b and r.z per tile
 // (compute.rs:226-331). Per-system results are formed by flush_upd.
+// Per tile the consumers pass two barriers: the stage wait (which also
+// separates the previous tile's warp partials from their publication by
+// thread 0) and the one between the block solves and the z writes.
 template <bool kInit>
 __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, StepParams *sp, float *smem) {
-    __shared__ __align__(8) uint64_t full[2], empty[2];
-    __shared__ UpdDesc desc[2];
+    constexpr uint32_t NS = kUpdStages;
+    __shared__ __align__(8) uint64_t full[NS], empty[NS];
+    __shared__ UpdDesc desc[NS];
+    __shared__ UpdDesc bdesc[32];
     __shared__ float sz[kTileRows];
     __shared__ uint32_t sflag[kTileRows];
     __shared__ double red[64];
-    __shared__ int s_last, s_ok;
+    __shared__ double2 wred[2 * (kThreads / 32)];
+    __shared__ int s_last, s_ok[2];
     const uint32_t tid = threadIdx.x;
     if (tid == 0) {
-        mbar_init(&full[0], 1);
-        mbar_init(&full[1], 1);
-        mbar_init(&empty[0], kThreads);
-        mbar_init(&empty[1], kThreads);
+        for (uint32_t i = 0; i < NS; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], kThreads / 32);
+        }
         fence_barrier_init();
     }
+    if (tid < kTileRows) sflag[tid] = 0u;
     __syncthreads();
     if (tid >= kThreads) {
-        if (tid != kThreads) return;
-        uint32_t w = blockIdx.x;
-        for (uint32_t k = 0;; ++k) {
-            const uint32_t s = k & 1u;
-            if (k >= 2 && !mbar_wait(&empty[s], ((k >> 1) - 1) & 1u)) {
-                atomicOr(&sp->error, 32u);
-                return;
-            }
-            UpdDesc d;
-            d.valid = resolve_upd<kInit>(sys, sp, &w, &d) ? 1u : 0u;
-            desc[s] = d;
-            if (d.valid) {
-                issue_upd<kInit>(sys, d, smem + s * kUpdStageFloats, &full[s]);
-            } else {
-                mbar_expect_tx(&full[s], 0);
-                return;
-            }
-        }
+        if (tid < kThreads + 32) upd_producer<kInit>(sys, sp, smem, full, empty, desc, bdesc);
+        return;
     }
-    uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles published since the last ticket
+    uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles of run_sys published since the last ticket
+    uint32_t pend_sys = 0, pend_tile = 0;         // thread 0: tile whose warp partials wait in wred
+    bool pend = false;
     for (uint32_t k = 0;; ++k) {
-        const uint32_t s = k & 1u;
-        if (!consumer_wait(&full[s], (k >> 1) & 1u, &s_ok)) {
-            if (tid == 0) {
-                atomicOr(&sp->error, kInit ? 4u : 2u);
-                mbar_wait(&full[s ^ 1u], ((k + 1) >> 1) & 1u);  // bounded drain of the other stage
-            }
+        const uint32_t s = k % NS, par = (k / NS) & 1u;
+        if (tid == 0) s_ok[k & 1u] = mbar_wait(&full[s], par) ? 1 : 0;
+        csync();
+        if (!s_ok[k & 1u]) {
+            if (tid == 0) atomicOr(&sp->error, kInit ? 4u : 2u);
             return;
         }
+        mbar_wait(&full[s], par);  // completed: acquire in every thread
         const UpdDesc d = desc[s];
+        if (tid == 0 && pend) {
+            const double2 *wr = wred + 8 * ((k - 1) & 1u);
+            double va = 0.0, vb = 0.0;
+#pragma unroll
+            for (int q = 0; q < kThreads / 32; ++q) {
+                va += wr[q].x;
+                vb += wr[q].y;
+            }
+            sys[pend_sys].part_b[pend_tile] = make_double2(va, vb);
+            pend = false;
+        }
         if (!d.valid) break;
-        const SysDesc &S = sys[d.sys];
-        float *stage = smem + s * kUpdStageFloats;
-        const uint32_t o = d.row0 - d.ra + tid;
-        float ri = 0.0f;
-        double da = 0.0;  // loop: r.r; init: b.b
-        sflag[tid] = 0u;
-        if (tid < d.rows) {
-            const uint32_t i = d.row0 + tid;
-            if (kInit) {
-                const float bi = stage[o];
-                ri = __fsub_rn(bi, stage[3 * kVecCap + o]);
-                da = (double)bi * (double)bi;
-            } else {
-                const float a = d.alpha, ma = -a;
-                float xi = stage[o];
-                ri = stage[2 * kVecCap + o];
-                xi = __fadd_rn(xi, __fmul_rn(a, stage[kVecCap + o]));
-                ri = __fadd_rn(ri, __fmul_rn(ma, stage[3 * kVecCap + o]));
-                S.x[i] = xi;
-                da = (double)ri * (double)ri;
-            }
-            S.r[i] = ri;
-            stage[2 * kVecCap + o] = ri;
-        }
-        csync();
-        bj_stage(d, stage, sz, sflag);
-        csync();
-        // The stage is no longer read: hand it back to the producer.
-        fence_proxy_async();
-        mbar_arrive(&empty[s]);
-        double rz = 0.0;
-        if (tid < d.rows) {
-            const uint32_t i = d.row0 + tid;
-            float zi;
-            if (sflag[tid]) {
-                zi = sz[tid];
-                S.z[i] = zi;
-            } else {
-                zi = S.z[i];
-            }
-            if (kInit) S.p[i] = zi;
-            rz = (double)ri * (double)zi;
-        }
-        const double2 tot = block_sum2(da, rz, red);
         if (d.sys != run_sys) {
             flush_upd<kInit>(sys, sp, run_sys, run_cnt, red, &s_last);
             run_sys = d.sys;
             run_cnt = 0;
         }
-        if (tid == 0) S.part_b[d.tile] = tot;
+        const SysDesc &S = sys[d.sys];
+        float *stage = smem + s * kUpdStageFloats;
+        const uint32_t o = d.row0 - d.ra + tid;
+        const float ma = -d.alpha;
+        float ri = 0.0f;
+        double da = 0.0;  // loop: r.r; init: b.b
+        if (tid < d.rows) {
+            const uint32_t i = d.row0 + tid;
+            ri = staged_r<kInit>(stage, o, ma);
+            if (kInit) {
+                const float bi = stage[o];
+                da = (double)bi * (double)bi;
+            } else {
+                const float xi = __fadd_rn(stage[o], __fmul_rn(d.alpha, stage[kVecCap + o]));
+                S.x[i] = xi;
+                da = (double)ri * (double)ri;
+            }
+            S.r[i] = ri;
+        }
+        const uint32_t tag = k + 1;
+        bj_stage<kInit>(d, stage, sz, sflag, tag);
+        // Every thread is done with the stage: hand it back to the producer.
+        fence_proxy_async();
+        mbar_arrive_warp(&empty[s]);
+        csync();
+        double rz = 0.0;
+        if (tid < d.rows) {
+            const uint32_t i = d.row0 + tid;
+            float zi;
+            if (sflag[tid] == tag) {
+                zi = sz[tid];
+                S.z[i] = zi;
+            } else {
+                zi = S.z[i];  // a row the block solve leaves alone (position >= 6 in its block)
+            }
+            if (kInit) S.p[i] = zi;
+            rz = (double)ri * (double)zi;
+        }
+        da = warp_sum(da);
+        rz = warp_sum(rz);
+        if ((tid & 31u) == 0) wred[8 * (k & 1u) + (tid >> 5)] = make_double2(da, rz);
+        pend = true;
+        pend_sys = d.sys;
+        pend_tile = d.tile;
         ++run_cnt;
     }
     if (run_sys != 0xffffffffu) flush_upd<kInit>(sys, sp, run_sys, run_cnt, red, &s_last);
@@ -761,17 +1029,17 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
 
 }  // namespace
 
-__global__ void __launch_bounds__(kPipeThreads, 3) k_spmv_loop(const SysDesc *__restrict__ sys, StepParams *sp) {
+__global__ void __launch_bounds__(kSpmvThreads, 3) k_spmv_loop(const SysDesc *__restrict__ sys, StepParams *sp) {
     extern __shared__ __align__(128) float smem[];
     spmv_pipeline<M_LOOP>(sys, sp, nullptr, nullptr, smem);
 }
 
-__global__ void __launch_bounds__(kPipeThreads, 3) k_spmv_init(const SysDesc *__restrict__ sys, StepParams *sp) {
+__global__ void __launch_bounds__(kSpmvThreads, 3) k_spmv_init(const SysDesc *__restrict__ sys, StepParams *sp) {
     extern __shared__ __align__(128) float smem[];
     spmv_pipeline<M_INIT>(sys, sp, nullptr, nullptr, smem);
 }
 
-__global__ void __launch_bounds__(kPipeThreads, 3) k_spmv_plain(const SysDesc *__restrict__ sys, StepParams *sp,
+__global__ void __launch_bounds__(kSpmvThreads, 3) k_spmv_plain(const SysDesc *__restrict__ sys, StepParams *sp,
                                                          const float *__restrict__ x, float *__restrict__ y) {
     extern __shared__ __align__(128) float smem[];
     spmv_pipeline<M_PLAIN>(sys, sp, x, y, smem);

@@ -17,20 +17,24 @@
 
 namespace wsb {
 
-// Shared-memory stages (floats) of the two TMA-pipelined kernels; each
-// kernel double-buffers its stage.
-// SpMV stage: CSR values + columns, or BSR6 block values + block columns +
-// gathered x, then the row pointers at kSpmvRpOff.
-constexpr int kSpmvDataFloats = (2 * (kCsrCap + 8) > 43 * kBsrCapBlocks + 8) ? 2 * (kCsrCap + 8)
-                                                                             : 43 * kBsrCapBlocks + 8;
-constexpr int kSpmvRpOff = (kSpmvDataFloats + 3) & ~3;
+// Shared-memory stages (floats) of the two TMA-pipelined kernels. The SpMV
+// runs a ring of kSpmvStages stages, the update kernel kUpdStages.
+// SpMV stage: CSR values [0, kCsrCap+8) and columns [kCsrCap+8, 2(kCsrCap+8)),
+// or BSR6 block values [0, 36 cap), block columns, then the gathered x (6 per
+// block); the row pointers at kSpmvRpOff.
+constexpr int kSpmvBcolOff = 36 * kBsrCapBlocks;
+constexpr int kSpmvXgOff = kSpmvBcolOff + kBsrCapBlocks + 8;
+constexpr int kSpmvBsrEnd = kSpmvXgOff + 6 * kBsrCapBlocks;
+constexpr int kSpmvCsrEnd = 2 * (kCsrCap + 8);
+constexpr int kSpmvRpOff = (((kSpmvCsrEnd > kSpmvBsrEnd) ? kSpmvCsrEnd : kSpmvBsrEnd) + 3) & ~3;
 constexpr int kSpmvStageFloats = ((kSpmvRpOff + kTileRows + 8) + 31) & ~31;
 constexpr int kUpdStageFloats = ((4 * (kTileRows + 8) + kUpdBlocks * 36 + kUpdBlocks + 8) + 31) & ~31;
 // Threads per CTA of the TMA-pipelined kernels: kThreads consumers plus one
-// producer warp.
+// producer warp (update), plus a gather warp (SpMV).
 constexpr int kPipeThreads = kThreads + 32;
-constexpr size_t kSpmvSmem = 2 * (size_t)kSpmvStageFloats * sizeof(float);
-constexpr size_t kUpdSmem = 2 * (size_t)kUpdStageFloats * sizeof(float);
+constexpr int kSpmvThreads = kThreads + 64;
+constexpr size_t kSpmvSmem = (size_t)kSpmvStages * kSpmvStageFloats * sizeof(float);
+constexpr size_t kUpdSmem = (size_t)kUpdStages * kUpdStageFloats * sizeof(float);
 
 // k_spmv_loop: Ap = A p with p.Ap and alpha; k_spmv_init: Ap = A x.
 __global__ void k_spmv_loop(const SysDesc *__restrict__ sys, StepParams *sp);

@@ -19,11 +19,29 @@ namespace wsb {
 // ---------------------------------------------------------------------------
 // Launch geometry shared by host and device code.
 // ---------------------------------------------------------------------------
+// The SpMV tile caps and ring depth can be overridden at build time
+// (-DWSB_CSR_CAP=..., -DWSB_BSR_CAP=..., -DWSB_SPMV_STAGES=...) for tuning
+// sweeps; the host tiling and the kernels always use the same values.
+#ifndef WSB_CSR_CAP
+#define WSB_CSR_CAP 4096
+#endif
+#ifndef WSB_BSR_CAP
+#define WSB_BSR_CAP 192
+#endif
+#ifndef WSB_SPMV_STAGES
+#define WSB_SPMV_STAGES 2
+#endif
+#ifndef WSB_UPD_STAGES
+#define WSB_UPD_STAGES 3
+#endif
 constexpr int kThreads = 256;        // threads per CTA for every solver kernel
 constexpr int kTileRows = 256;       // rows (or block rows x 6) per tile, <= kThreads
-constexpr int kCsrCap = 4096;        // CSR nonzeros per SpMV tile (one TMA stage)
-constexpr int kBsrCapBlocks = 192;   // BSR 6x6 blocks per SpMV tile (27 KiB of values)
+constexpr int kCsrCap = WSB_CSR_CAP;         // CSR nonzeros per SpMV tile (one TMA stage)
+constexpr int kBsrCapBlocks = WSB_BSR_CAP;   // BSR 6x6 blocks per SpMV tile (144 B each)
+constexpr int kSpmvStages = WSB_SPMV_STAGES; // depth of the SpMV shared-memory ring
 constexpr int kUpdBlocks = 64;       // block-Jacobi blocks per update tile
+constexpr int kUpdStages = WSB_UPD_STAGES;   // depth of the update shared-memory ring
+static_assert(kCsrCap % 4 == 0 && kBsrCapBlocks % 4 == 0 && kSpmvStages >= 2, "SpMV tile caps");
 constexpr int kChunkRows = 4096;     // rows per work item of the vector kernels
 constexpr int kPadElems = 64;        // tail padding of streamed arrays (elements)
 
