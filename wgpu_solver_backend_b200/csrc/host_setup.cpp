@@ -176,7 +176,7 @@ int validate_system(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, ui
     return WSB_OK;
 }
 
-// Greedy CSR row tiles: <= kTileRows rows and <= kCsrCap nonzeros (one TMA
+// Greedy CSR row tiles: <= kSpmvTileRows rows and <= kCsrCap nonzeros (one TMA
 // stage), except a single row longer than kCsrCap, which gets a tile of its
 // own and is streamed through shared memory in chunks by the kernel.
 void build_spmv_tiles_csr(uint32_t n, const uint32_t *row_ptr, std::vector<SpmvTile> *out) {
@@ -184,7 +184,7 @@ void build_spmv_tiles_csr(uint32_t n, const uint32_t *row_ptr, std::vector<SpmvT
     uint32_t r0 = 0;
     while (r0 < n) {
         uint32_t r1 = r0;
-        while (r1 < n && r1 - r0 < (uint32_t)kTileRows) {
+        while (r1 < n && r1 - r0 < (uint32_t)kSpmvTileRows) {
             const uint64_t tile_nnz = (uint64_t)row_ptr[r1 + 1] - row_ptr[r0];
             if (r1 > r0 && tile_nnz > (uint64_t)kCsrCap) break;
             ++r1;
@@ -195,11 +195,11 @@ void build_spmv_tiles_csr(uint32_t n, const uint32_t *row_ptr, std::vector<SpmvT
     }
 }
 
-// BSR6 tiles over block rows: <= kTileRows/6 block rows and <= kBsrCapBlocks
+// BSR6 tiles over block rows: <= kSpmvTileRows/6 block rows and <= kBsrCapBlocks
 // blocks (a longer block row is chunked by the kernel).
 void build_spmv_tiles_bsr(uint32_t nbrows, const uint32_t *brow_ptr, std::vector<SpmvTile> *out) {
     out->clear();
-    const uint32_t max_brows = kTileRows / 6;
+    const uint32_t max_brows = kSpmvTileRows / 6;
     uint32_t r0 = 0;
     while (r0 < nbrows) {
         uint32_t r1 = r0;

@@ -91,6 +91,17 @@ __device__ __forceinline__ void cp_async_mbar_arrive(uint64_t *bar) {
     asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// Non-blocking probe of a phase.
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\tmbarrier.test_wait.parity.shared::cta.b64 P, [%1], %2;\n\tselp.u32 %0, 1, 0, P;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
@@ -111,6 +122,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     return true;
 }
 
+// A phase that another thread of the CTA has already seen complete: a
+// non-blocking check (which also makes the phase's data visible to this
+// thread), with the bounded wait as a fallback.
+__device__ __forceinline__ void mbar_observe(uint64_t *bar, uint32_t parity) {
+    if (!mbar_test_wait(bar, parity)) mbar_wait(bar, parity);
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -129,7 +147,10 @@ __device__ __forceinline__ void mbar_arrive_warp(uint64_t *bar) {
 // themselves on named barrier 1 so the other warps never have to join. Kernels without a
 // producer warp launch exactly kThreads threads and use the same barrier.
 
-__device__ __forceinline__ void csync() { asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory"); }
+template <int N = kThreads>
+__device__ __forceinline__ void csync() {
+    asm volatile("bar.sync 1, %0;" ::"n"(N) : "memory");
+}
 
 // ---------------------------------------------------------------------------
 // Reductions
@@ -140,21 +161,24 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// Fixed-shape block reduction (result valid in thread 0). red: >= 32 doubles.
+// Fixed-shape block reduction over the N consumer threads (result valid in
+// thread 0). red: >= 32 doubles.
+template <int N = kThreads>
 __device__ __forceinline__ double block_sum(double v, double *red) {
     v = warp_sum(v);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (lane == 0) red[w] = v;
-    csync();
+    csync<N>();
     double s = 0.0;
     if (w == 0) {
-        s = lane < (kThreads >> 5) ? red[lane] : 0.0;
+        s = lane < (N >> 5) ? red[lane] : 0.0;
         s = warp_sum(s);
     }
-    csync();
+    csync<N>();
     return s;
 }
 
+template <int N = kThreads>
 __device__ __forceinline__ double2 block_sum2(double a, double b, double *red) {
     a = warp_sum(a);
     b = warp_sum(b);
@@ -163,67 +187,71 @@ __device__ __forceinline__ double2 block_sum2(double a, double b, double *red) {
         red[w] = a;
         red[32 + w] = b;
     }
-    csync();
+    csync<N>();
     double sa = 0.0, sb = 0.0;
     if (w == 0) {
-        sa = lane < (kThreads >> 5) ? red[lane] : 0.0;
-        sb = lane < (kThreads >> 5) ? red[32 + lane] : 0.0;
+        sa = lane < (N >> 5) ? red[lane] : 0.0;
+        sb = lane < (N >> 5) ? red[32 + lane] : 0.0;
         sa = warp_sum(sa);
         sb = warp_sum(sb);
     }
-    csync();
+    csync<N>();
     return make_double2(sa, sb);
 }
 
-// Sum of n FP64 partials over the consumer threads: thread t adds elements
-// t, t + kThreads, t + 2 kThreads, ... in that order (16 loads in flight),
-// then the fixed-shape block sum. Result valid in thread 0.
+// Sum of n FP64 partials over the N consumer threads: thread t adds
+// elements t, t + N, t + 2N, ... in that order (16 loads in flight), then the
+// fixed-shape block sum. Result valid in thread 0.
+template <int N = kThreads>
 __device__ __forceinline__ double sum_partials(const double *__restrict__ p, uint32_t n, double *red) {
     double v = 0.0;
     uint32_t i = threadIdx.x;
-    for (; i + 15u * kThreads < n; i += 16u * kThreads) {
+    for (; i + 15u * N < n; i += 16u * N) {
         double q[16];
 #pragma unroll
-        for (int u = 0; u < 16; ++u) q[u] = __ldcg(p + i + u * kThreads);
+        for (int u = 0; u < 16; ++u) q[u] = __ldcg(p + i + u * N);
 #pragma unroll
         for (int u = 0; u < 16; ++u) v += q[u];
     }
-    for (; i < n; i += kThreads) v += __ldcg(p + i);
-    return block_sum(v, red);
+    for (; i < n; i += N) v += __ldcg(p + i);
+    return block_sum<N>(v, red);
 }
 
 // The same for pairs of partials (both components in one pass).
+template <int N = kThreads>
 __device__ __forceinline__ double2 sum_partials2(const double2 *__restrict__ p, uint32_t n, double *red) {
     double va = 0.0, vb = 0.0;
     uint32_t i = threadIdx.x;
-    for (; i + 7u * kThreads < n; i += 8u * kThreads) {
+    for (; i + 7u * N < n; i += 8u * N) {
         double2 q[8];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) q[u] = __ldcg(p + i + u * kThreads);
+        for (int u = 0; u < 8; ++u) q[u] = __ldcg(p + i + u * N);
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             va += q[u].x;
             vb += q[u].y;
         }
     }
-    for (; i < n; i += kThreads) {
+    for (; i < n; i += N) {
         const double2 q = __ldcg(p + i);
         va += q.x;
         vb += q.y;
     }
-    return block_sum2(va, vb, red);
+    return block_sum2<N>(va, vb, red);
 }
 
 // Ticket on a per-system counter: this CTA adds the number of tiles whose
-// partials it has published (thread 0 wrote them); true in every thread of
-// the CTA whose tickets complete the system's total.
-__device__ __forceinline__ bool take_ticket(uint32_t *counter, uint32_t cnt, uint32_t total, int *s_last) {
-    if (threadIdx.x == 0) {
+// partials it has published (thread `who` wrote them and takes the ticket);
+// true in every thread of the CTA whose tickets complete the system's total.
+template <int N = kThreads>
+__device__ __forceinline__ bool take_ticket(uint32_t *counter, uint32_t cnt, uint32_t total, int *s_last,
+                                            uint32_t who = 0) {
+    if (threadIdx.x == who) {
         __threadfence();
         const uint32_t t = atomicAdd(counter, cnt);
         *s_last = (t + cnt == total);
     }
-    csync();
+    csync<N>();
     const bool last = *s_last != 0;
     if (last) __threadfence();
     return last;
@@ -238,6 +266,7 @@ enum SpmvMode { M_LOOP = 0, M_INIT = 1, M_PLAIN = 2 };
 // columns at kColOff; BSR6 block values [0, 36 kBsrCapBlocks), block columns
 // at kBcolOff, gathered x at kXgOff (float2, 3 per block); row pointers at
 // kRpOff.
+constexpr int NC = kSpmvConsumers;  // consumer threads of the SpMV kernels
 constexpr int kValCap = kCsrCap + 8;
 constexpr int kColOff = kValCap;
 constexpr int kBcolOff = kSpmvBcolOff;
@@ -246,36 +275,56 @@ constexpr int kRpOff = kSpmvRpOff;
 static_assert((kColOff * 4) % 16 == 0 && (kBcolOff * 4) % 16 == 0 && (kXgOff * 4) % 16 == 0 &&
                   (kRpOff * 4) % 16 == 0 && (kSpmvStageFloats * 4) % 128 == 0,
               "TMA alignment");
-static_assert(kSpmvStageFloats >= kRpOff + kTileRows + 8, "stage size");
+static_assert(kSpmvStageFloats >= kRpOff + kSpmvTileRows + 8, "stage size");
 
 struct SpmvDesc {
     uint32_t valid, sys, tile, layout;
     uint32_t r0, nr;  // tile rows in layout units (rows, or block rows)
     uint32_t k0, k1;  // nonzero (block) range
-    uint32_t ka, ra;  // 4-aligned starts of the staged column / row-pointer ranges
+    uint32_t ka;      // 4-aligned start of the staged CSR value / column range
     uint32_t lng;     // a single row longer than a stage: synchronous path
-    uint32_t pad;
+    const float *x;   // the vector multiplied: p (loop), x0 (init) or the caller's x
+    float *y;         // Ap (loop, init) or the caller's y
+    double *part;     // the system's per-tile p.Ap partials (loop)
+    const uint32_t *rptr;  // the tile's row pointers: row_ptr + r0 or brow_ptr + r0
+    const uint32_t *cols;  // BSR6: the tile's block columns, bcol + k0
+    const float *vsrc;     // bulk-copy source of the values: bval + 36 k0, or val + ka
+    const uint32_t *csrc;  // CSR: bulk-copy source of the columns, col + ka
 };
 
-// Resolves one work index of the SpMV work list (one producer lane). False
-// for an index past the end, an invalid item (which also sets an error code)
-// and, in the loop kernel, a system that is no longer active.
 template <int kMode>
-__device__ __forceinline__ bool resolve_spmv(const SysDesc *__restrict__ sys, const StepParams *sp, uint32_t idx,
-                                             uint32_t nw, WorkItem it, SpmvDesc *d) {
+__device__ __forceinline__ const float *spmv_input(const SysDesc &S, const float *__restrict__ xplain) {
+    return kMode == M_PLAIN ? xplain : kMode == M_INIT ? S.x : S.p;
+}
+
+// Checks one work index of the SpMV work list (one producer lane): false
+// for an index past the end, an invalid item (which also sets an error code)
+// and, in the loop kernel, a system that is no longer active. *it is set to
+// the (system, tile) the index stands for.
+template <int kMode>
+__device__ __forceinline__ bool check_spmv(const SysDesc *__restrict__ sys, const StepParams *sp, uint32_t idx,
+                                           uint32_t nw, WorkItem *it) {
     if (idx >= nw) return false;
     if (kMode == M_PLAIN) {
-        it.sys = 0;
-        it.tile = idx;
-    } else {
-        if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_stiles) {
-            atomicOr(const_cast<uint32_t *>(&sp->error), 8u);  // invalid work item: skipped
-            return false;
-        }
-        if (kMode == M_LOOP && !sys[it.sys].st->active) return false;
+        it->sys = 0;
+        it->tile = idx;
+        return true;
     }
+    if (it->sys >= sp->num_sys || it->tile >= sys[it->sys].n_stiles) {
+        atomicOr(const_cast<uint32_t *>(&sp->error), 8u);  // invalid work item: skipped
+        return false;
+    }
+    return !(kMode == M_LOOP && !sys[it->sys].st->active);
+}
+
+// Fills the descriptor of a checked work item, field by field, in shared memory.
+template <int kMode>
+__device__ __forceinline__ void fill_spmv(const SysDesc *__restrict__ sys, WorkItem it, const float *xplain,
+                                          float *yplain, SpmvDesc *d) {
     const SysDesc &S = sys[it.sys];
     const SpmvTile T = S.stiles[it.tile];
+    const bool bsr = S.layout == LAYOUT_BSR6;
+    const uint32_t ka = T.k0 & ~3u;
     d->valid = 1;
     d->sys = it.sys;
     d->tile = it.tile;
@@ -284,56 +333,77 @@ __device__ __forceinline__ bool resolve_spmv(const SysDesc *__restrict__ sys, co
     d->nr = T.row1 - T.row0;
     d->k0 = T.k0;
     d->k1 = T.k1;
-    d->ka = T.k0 & ~3u;
-    d->ra = T.row0 & ~3u;
-    d->lng = (S.layout == LAYOUT_BSR6) ? (T.k1 - T.k0 > (uint32_t)kBsrCapBlocks) : (T.k1 - T.k0 > (uint32_t)kCsrCap);
-    return true;
+    d->ka = ka;
+    d->lng = bsr ? (T.k1 - T.k0 > (uint32_t)kBsrCapBlocks) : (T.k1 - T.k0 > (uint32_t)kCsrCap);
+    d->x = spmv_input<kMode>(S, xplain);
+    d->y = kMode == M_PLAIN ? yplain : S.ap;
+    d->part = S.part_a;
+    d->rptr = (bsr ? S.brow_ptr : S.row_ptr) + T.row0;
+    d->cols = bsr ? S.bcol + T.k0 : nullptr;
+    d->vsrc = bsr ? S.bval + (size_t)T.k0 * 36u : S.val + ka;
+    d->csrc = bsr ? nullptr : S.col + ka;
 }
 
-// Issues the bulk copies of a resolved tile into a stage (producer lane 0).
-__device__ __forceinline__ void issue_spmv(const SysDesc *__restrict__ sys, const SpmvDesc &d, float *stage,
-                                           uint64_t *bar, uint64_t pol) {
+// Issues the bulk copies of a resolved tile into a stage (producer lane 0):
+// the block values (BSR6) or the values and columns (CSR). Row pointers and
+// block columns are read by the gather warps.
+__device__ __forceinline__ void issue_spmv(const SpmvDesc &d, float *stage, uint64_t *bar, uint64_t pol) {
     if (d.lng) {
         mbar_expect_tx(bar, 0);
         return;
     }
-    const SysDesc &S = sys[d.sys];
-    const uint32_t rc = ((d.r0 + d.nr + 1 - d.ra) + 3) & ~3u;
-    const uint32_t cc = ((d.k1 - d.ka) + 3) & ~3u;
-    uint32_t *rp = reinterpret_cast<uint32_t *>(stage + kRpOff);
     if (d.layout == LAYOUT_BSR6) {
         const uint32_t vb = (d.k1 - d.k0) * 144u;
-        mbar_expect_tx(bar, vb + 4u * cc + 4u * rc);
-        if (vb) tma_load_stream(stage, S.bval + (size_t)d.k0 * 36u, vb, bar, pol);
-        if (cc) tma_load_stream(stage + kBcolOff, S.bcol + d.ka, 4u * cc, bar, pol);
-        tma_load_stream(rp, S.brow_ptr + d.ra, 4u * rc, bar, pol);
+        mbar_expect_tx(bar, vb);
+        if (vb) tma_load_stream(stage, d.vsrc, vb, bar, pol);
     } else {
-        mbar_expect_tx(bar, 8u * cc + 4u * rc);
+        const uint32_t cc = ((d.k1 - d.ka) + 3) & ~3u;
+        mbar_expect_tx(bar, 8u * cc);
         if (cc) {
-            tma_load_stream(stage, S.val + d.ka, 4u * cc, bar, pol);
-            tma_load_stream(stage + kColOff, S.col + d.ka, 4u * cc, bar, pol);
+            tma_load_stream(stage, d.vsrc, 4u * cc, bar, pol);
+            tma_load_stream(stage + kColOff, d.csrc, 4u * cc, bar, pol);
         }
-        tma_load_stream(rp, S.row_ptr + d.ra, 4u * rc, bar, pol);
     }
 }
 
-// Gather warp, BSR6 tile in a filled stage: the 6 x values of every block
-// column into the stage's gather area as 3 float2 per block (cp.async, no
-// registers held, so the warp moves on to the next tile at once).
-__device__ __forceinline__ void gather_bsr(const SpmvDesc &d, const float *__restrict__ xin, float *stage,
-                                           uint32_t lane) {
+// Gather warp, one tile (32 lanes): the tile's row pointers into the stage
+// (rp[i] = row_ptr[r0 + i], i <= nr), and for BSR6 its block columns (bcol[i]
+// = block column of block k0 + i) and the 6 x values of every block column,
+// as 3 float2 per block, by cp.async. None of this waits for the tile's bulk
+// copy, so the gathers run while the block values stream in.
+__device__ __forceinline__ void gather_tile(const SpmvDesc &d, float *stage, uint32_t lane) {
+    uint32_t *rp = reinterpret_cast<uint32_t *>(stage + kRpOff);
+    for (uint32_t i = lane; i <= d.nr; i += 32u) rp[i] = __ldg(d.rptr + i);
+    if (d.layout != LAYOUT_BSR6) return;
+    const float *__restrict__ xin = d.x;
     const bool al8 = (reinterpret_cast<uintptr_t>(xin) & 7u) == 0;
-    const uint32_t *bcol = reinterpret_cast<const uint32_t *>(stage + kBcolOff);
+    uint32_t *bcol = reinterpret_cast<uint32_t *>(stage + kBcolOff);
     float *xg = stage + kXgOff;
-    const uint32_t cofs = d.k0 - d.ka, ne = 3u * (d.k1 - d.k0);
-    for (uint32_t e = lane; e < ne; e += 32u) {
-        const uint32_t blk = e / 3u, h = e - 3u * blk;
-        const float *src = xin + 6u * (size_t)bcol[blk + cofs] + 2u * h;
-        if (al8) {
-            cp_async8(xg + 2u * e, src);
-        } else {  // a caller's x that is only 4-byte aligned (plain SpMV entry point)
-            cp_async4(xg + 2u * e, src);
-            cp_async4(xg + 2u * e + 1u, src + 1);
+    const uint32_t nb = d.k1 - d.k0;
+    // All block columns of this lane first (independent loads), then the
+    // copies that depend on them.
+    constexpr int kPer = (kBsrCapBlocks + 31) / 32;
+    uint32_t c[kPer];
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+        const uint32_t blk = lane + 32u * q;
+        c[q] = blk < nb ? __ldg(d.cols + blk) : 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+        const uint32_t blk = lane + 32u * q;
+        if (blk < nb) {
+            bcol[blk] = c[q];
+            const float *src = xin + 6u * (size_t)c[q];
+            float *dst = xg + 6u * blk;
+            if (al8) {
+                cp_async8(dst, src);
+                cp_async8(dst + 2, src + 2);
+                cp_async8(dst + 4, src + 4);
+            } else {  // a caller's x that is only 4-byte aligned (plain SpMV entry point)
+#pragma unroll
+                for (int h = 0; h < 6; ++h) cp_async4(dst + h, src + h);
+            }
         }
     }
 }
@@ -347,18 +417,18 @@ __device__ __forceinline__ float csr_stage(const SpmvDesc &d, const float *__res
     const uint32_t *rp = reinterpret_cast<const uint32_t *>(stage + kRpOff);
     const uint32_t j0 = d.k0 - d.ka, j1 = d.k1 - d.ka;
     uint32_t j = j0 + threadIdx.x;
-    for (; j + 7 * kThreads < j1; j += 8 * kThreads) {
+    for (; j + 7 * NC < j1; j += 8 * NC) {
         float xv[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) xv[q] = __ldg(xin + col[j + q * kThreads]);
+        for (int q = 0; q < 8; ++q) xv[q] = __ldg(xin + col[j + q * NC]);
 #pragma unroll
-        for (int q = 0; q < 8; ++q) val[j + q * kThreads] = __fmul_rn(val[j + q * kThreads], xv[q]);
+        for (int q = 0; q < 8; ++q) val[j + q * NC] = __fmul_rn(val[j + q * NC], xv[q]);
     }
-    for (; j < j1; j += kThreads) val[j] = __fmul_rn(val[j], __ldg(xin + col[j]));
-    csync();
+    for (; j < j1; j += NC) val[j] = __fmul_rn(val[j], __ldg(xin + col[j]));
+    csync<NC>();
     float acc = 0.0f;
     if (threadIdx.x < d.nr) {
-        const uint32_t o = d.r0 - d.ra + threadIdx.x;
+        const uint32_t o = threadIdx.x;
         const uint32_t s = rp[o] - d.ka, e = rp[o + 1] - d.ka;
         for (uint32_t q = s; q < e; ++q) acc = __fadd_rn(acc, val[q]);
     }
@@ -382,25 +452,39 @@ __device__ __forceinline__ float bsr_stage(const SpmvDesc &d, const float *stage
     const uint32_t t = threadIdx.x;
     if (t < 6u * d.nr) {
         const uint32_t br = t / 6u, a = t - 6u * br;
-        const uint32_t o = d.r0 - d.ra + br;
-        const uint32_t s0 = rp[o] - d.k0, s1 = rp[o + 1] - d.k0;
-        const uint32_t cofs = d.k0 - d.ka, self = d.r0 + br;
+        const uint32_t s0 = rp[br] - d.k0, s1 = rp[br + 1] - d.k0;
+        const uint32_t self = d.r0 + br;
+        // The next block's operands are loaded before this block's products
+        // are added, so shared-memory latency overlaps the add chain.
+        float2 b0, b1, b2, x0, x1, x2;
+        uint32_t c = 0;
+        if (s0 < s1) {
+            const float2 *B = reinterpret_cast<const float2 *>(stage + s0 * 36u + a * 6u);
+            const float2 *X = xg + s0 * 3u;
+            b0 = B[0], b1 = B[1], b2 = B[2], x0 = X[0], x1 = X[1], x2 = X[2];
+            if (kOwn) c = bcol[s0];
+        }
         for (uint32_t blk = s0; blk < s1; ++blk) {
-            const float2 *B = reinterpret_cast<const float2 *>(stage + blk * 36u + a * 6u);
-            const float2 *X = xg + blk * 3u;
-            const float2 b0 = B[0], b1 = B[1], b2 = B[2];
-            const float2 x0 = X[0], x1 = X[1], x2 = X[2];
+            float2 nb0 = b0, nb1 = b1, nb2 = b2, nx0 = x0, nx1 = x1, nx2 = x2;
+            uint32_t nc = c;
+            if (blk + 1 < s1) {
+                const float2 *B = reinterpret_cast<const float2 *>(stage + (blk + 1) * 36u + a * 6u);
+                const float2 *X = xg + (blk + 1) * 3u;
+                nb0 = B[0], nb1 = B[1], nb2 = B[2], nx0 = X[0], nx1 = X[1], nx2 = X[2];
+                if (kOwn) nc = bcol[blk + 1];
+            }
             acc = __fadd_rn(acc, __fmul_rn(b0.x, x0.x));
             acc = __fadd_rn(acc, __fmul_rn(b0.y, x0.y));
             acc = __fadd_rn(acc, __fmul_rn(b1.x, x1.x));
             acc = __fadd_rn(acc, __fmul_rn(b1.y, x1.y));
             acc = __fadd_rn(acc, __fmul_rn(b2.x, x2.x));
             acc = __fadd_rn(acc, __fmul_rn(b2.y, x2.y));
-            if (kOwn && bcol[blk + cofs] == self) {
+            if (kOwn && c == self) {
                 const float2 xs = a < 2u ? x0 : (a < 4u ? x1 : x2);
                 xo = (a & 1u) ? xs.y : xs.x;
                 found = true;
             }
+            b0 = nb0, b1 = nb1, b2 = nb2, x0 = nx0, x1 = nx1, x2 = nx2, c = nc;
         }
     }
     if (kOwn) {
@@ -422,9 +506,9 @@ __device__ __forceinline__ float long_tile(const SysDesc &S, const SpmvDesc &d, 
             const uint32_t nb = min(d.k1 - c0, (uint32_t)kBsrCapBlocks);
             const float4 *src = reinterpret_cast<const float4 *>(S.bval) + (size_t)c0 * 9u;
             float4 *dst = reinterpret_cast<float4 *>(stage);
-            for (uint32_t q = t; q < nb * 9u; q += kThreads) dst[q] = __ldcs(src + q);
-            for (uint32_t q = t; q < nb; q += kThreads) bcol[q] = __ldcs(S.bcol + c0 + q);
-            csync();
+            for (uint32_t q = t; q < nb * 9u; q += NC) dst[q] = __ldcs(src + q);
+            for (uint32_t q = t; q < nb; q += NC) bcol[q] = __ldcs(S.bcol + c0 + q);
+            csync<NC>();
             if (t < 6u) {
                 for (uint32_t blk = 0; blk < nb; ++blk) {
                     const float *B = stage + blk * 36u + t * 6u;
@@ -433,7 +517,7 @@ __device__ __forceinline__ float long_tile(const SysDesc &S, const SpmvDesc &d, 
                     for (int jj = 0; jj < 6; ++jj) acc = __fadd_rn(acc, __fmul_rn(B[jj], __ldg(xx + jj)));
                 }
             }
-            csync();
+            csync<NC>();
         }
         return acc;
     }
@@ -441,15 +525,20 @@ __device__ __forceinline__ float long_tile(const SysDesc &S, const SpmvDesc &d, 
     constexpr uint32_t kChunk = 2 * kCsrCap;
     for (uint32_t c0 = d.k0; c0 < d.k1; c0 += kChunk) {
         const uint32_t c1 = min(d.k1, c0 + kChunk);
-        for (uint32_t q = c0 + t; q < c1; q += kThreads)
+        for (uint32_t q = c0 + t; q < c1; q += NC)
             stage[q - c0] = __fmul_rn(__ldcs(S.val + q), __ldg(xin + __ldcs(S.col + q)));
-        csync();
+        csync<NC>();
         if (t == 0)
             for (uint32_t q = c0; q < c1; ++q) acc = __fadd_rn(acc, stage[q - c0]);
-        csync();
+        csync<NC>();
     }
     return acc;
 }
+
+// The consumer thread that publishes the per-tile p.Ap partials and takes the
+// system tickets: lane 0 of the last consumer warp, which has no rows in
+// most BSR6 tiles and so is free while the others compute.
+constexpr uint32_t kPublisher = NC - 32;
 
 // The last CTA of a system's SpMV tiles: p.Ap from the per-tile partials in
 // tile order, alpha = rz_old / pAp (0 when pAp == 0, as
@@ -459,8 +548,8 @@ __device__ __forceinline__ void flush_spmv(const SysDesc *__restrict__ sys, uint
     if (cnt == 0) return;
     const SysDesc &S = sys[s];
     SysState *st = S.st;
-    if (!take_ticket(&st->cnt_a, cnt, S.n_stiles, s_last)) return;
-    const double pap = sum_partials(S.part_a, S.n_stiles, red);
+    if (!take_ticket<NC>(&st->cnt_a, cnt, S.n_stiles, s_last, kPublisher)) return;
+    const double pap = sum_partials<NC>(S.part_a, S.n_stiles, red);
     if (threadIdx.x == 0) {
         const double alpha = pap != 0.0 ? st->rz_old / pap : 0.0;
         st->pap = pap;
@@ -470,22 +559,20 @@ __device__ __forceinline__ void flush_spmv(const SysDesc *__restrict__ sys, uint
     }
 }
 
-template <int kMode>
-__device__ __forceinline__ const float *spmv_input(const SysDesc &S, const float *__restrict__ xplain) {
-    return kMode == M_PLAIN ? xplain : kMode == M_INIT ? S.x : S.p;
-}
+
 
 // Producer warp of the SpMV ring. The warp resolves 32 work items at once
 // (one lane each: work item -> system -> tile), so the chain of dependent
 // loads behind a tile is paid once per 32 tiles, and keeps the work items of
 // the next batch in flight meanwhile. Lane 0 then walks the batch in order:
 // it claims stage k % NS once the consumers released tile k - NS, publishes
-// the tile's descriptor and issues its bulk copies. After the last tile it
-// publishes an end marker. Every wait is bounded; on a timeout lane 0 records
+// the tile's descriptor (meta barrier) and issues its bulk copies. After the
+// last tile it publishes one end marker per gather warp. Every wait is bounded; on a timeout lane 0 records
 // an error, waits (bounded) for its copies still in flight and returns.
 template <int kMode>
-__device__ __forceinline__ void spmv_producer(const SysDesc *__restrict__ sys, StepParams *sp, float *smem,
-                                              uint64_t *full, uint64_t *empty, SpmvDesc *desc, SpmvDesc *bdesc) {
+__device__ __forceinline__ void spmv_producer(const SysDesc *__restrict__ sys, StepParams *sp,
+                                              const float *xplain, float *yplain, float *smem, uint64_t *full,
+                                              uint64_t *meta, uint64_t *empty, SpmvDesc *desc, SpmvDesc *bdesc) {
     constexpr uint32_t NS = kSpmvStages;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t G = gridDim.x;
@@ -498,18 +585,18 @@ __device__ __forceinline__ void spmv_producer(const SysDesc *__restrict__ sys, S
     bool err = false;
     const uint64_t pol = l2_evict_first_policy();
     for (;;) {
-        SpmvDesc d;
-        const bool ok = resolve_spmv<kMode>(sys, sp, base + lane * G, nw, it, &d);
+        const bool ok = check_spmv<kMode>(sys, sp, base + lane * G, nw, &it);
         const uint32_t m = __ballot_sync(0xffffffffu, ok);
-        if (ok) bdesc[__popc(m & ((1u << lane) - 1u))] = d;
+        if (ok) fill_spmv<kMode>(sys, it, xplain, yplain, &bdesc[__popc(m & ((1u << lane) - 1u))]);
         const uint32_t cnt = __popc(m);
         base += 32u * G;
         const bool more = base < nw;
         if (kMode != M_PLAIN && base + lane * G < nw) it = work[base + lane * G];  // next batch, in flight
         __syncwarp();
         if (lane == 0) {
-            for (uint32_t i = 0; i <= cnt; ++i) {
-                if (i == cnt && more) break;
+            // After the last tile: one end marker for each gather warp.
+            const uint32_t n_out = more ? cnt : cnt + kGatherWarps;
+            for (uint32_t i = 0; i < n_out; ++i) {
                 const uint32_t s = k % NS;
                 if (k >= NS && !mbar_wait(&empty[s], ((k / NS) - 1) & 1u)) {
                     atomicOr(&sp->error, 16u);
@@ -518,10 +605,12 @@ __device__ __forceinline__ void spmv_producer(const SysDesc *__restrict__ sys, S
                 }
                 if (i < cnt) {
                     desc[s] = bdesc[i];
-                    issue_spmv(sys, bdesc[i], smem + s * kSpmvStageFloats, &full[s], pol);
+                    mbar_arrive(&meta[s]);  // the gather warps may start on this tile
+                    issue_spmv(desc[s], smem + s * kSpmvStageFloats, &full[s], pol);
                     issued = k + 1;
                 } else {  // end marker
                     desc[s].valid = 0;
+                    mbar_arrive(&meta[s]);
                     mbar_expect_tx(&full[s], 0);
                 }
                 ++k;
@@ -537,39 +626,40 @@ __device__ __forceinline__ void spmv_producer(const SysDesc *__restrict__ sys, S
     }
 }
 
-// Gather warp of the SpMV ring: follows the tiles as they land and, for
-// BSR6 tiles, gathers the x values of every block column into the stage
-// (cp.async); the stage's gather barrier completes when those copies have
-// landed (it completes at once for tiles that need no gather). The warp never
-// waits for its own copies, so it stays ahead of the consumers.
+// Gather warps of the SpMV ring (warp g takes tiles g, g + kGatherWarps, ...): as soon
+// as the producer publishes a tile's descriptor, the warp reads its row
+// pointers and block columns and issues the x gathers (cp.async), in
+// parallel with the tile's bulk copy. The stage's gather barrier completes
+// when the warp's stores are done (a release arrival per lane) and its
+// cp.async copies have landed (an asynchronous arrival per lane).
 template <int kMode>
 __device__ __forceinline__ void spmv_gatherer(const SysDesc *__restrict__ sys, StepParams *sp,
-                                              const float *__restrict__ xplain, float *smem, uint64_t *full,
-                                              uint64_t *gath, const SpmvDesc *desc) {
+                                              const float *__restrict__ xplain, float *smem, uint64_t *meta,
+                                              uint64_t *gath, const SpmvDesc *desc, uint32_t g) {
     constexpr uint32_t NS = kSpmvStages;
     const uint32_t lane = threadIdx.x & 31u;
-    for (uint32_t j = 0;; ++j) {
+    for (uint32_t j = g;; j += kGatherWarps) {
         const uint32_t s = j % NS, par = (j / NS) & 1u;
         uint32_t ok = 1;
-        if (lane == 0) ok = mbar_wait(&full[s], par) ? 1u : 0u;
+        if (lane == 0) ok = mbar_wait(&meta[s], par) ? 1u : 0u;
         ok = __shfl_sync(0xffffffffu, ok, 0);
         if (!ok) {
             if (lane == 0) atomicOr(&sp->error, 64u);
             break;
         }
-        mbar_wait(&full[s], par);  // completed: the stage and its descriptor are visible
+        mbar_wait(&meta[s], par);  // completed: the descriptor is visible
         const SpmvDesc d = desc[s];
-        if (d.valid && d.layout == LAYOUT_BSR6 && !d.lng)
-            gather_bsr(d, spmv_input<kMode>(sys[d.sys], xplain), smem + s * kSpmvStageFloats, lane);
+        if (d.valid && !d.lng) gather_tile(d, smem + s * kSpmvStageFloats, lane);
+        mbar_arrive(&gath[s]);
         cp_async_mbar_arrive(&gath[s]);
         if (!d.valid) break;
     }
     cp_async_wait<0>();
 }
 
-// The SpMV pipeline shared by the loop, init and plain kernels: kThreads
+// The SpMV pipeline shared by the loop, init and plain kernels: NC
 // consumer threads compute tile after tile from the ring that the producer
-// warp fills and the gather warp completes. Per tile the consumers pass one
+// warp fills and the gather warps complete. Per tile the consumers pass one
 // barrier (the stage wait, which also separates the previous tile's warp
 // partials from their publication by thread 0).
 template <int kMode>
@@ -577,56 +667,56 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
                                               const float *__restrict__ xplain, float *__restrict__ yplain,
                                               float *smem) {
     constexpr uint32_t NS = kSpmvStages;
-    __shared__ __align__(8) uint64_t full[NS], gath[NS], empty[NS];
+    __shared__ __align__(8) uint64_t full[NS], meta[NS], gath[NS], empty[NS];
     __shared__ SpmvDesc desc[NS];
     __shared__ SpmvDesc bdesc[32];
     __shared__ double red[64];
-    __shared__ double wred[2 * (kThreads / 32)];
+    __shared__ double wred[2 * (NC / 32)];
     __shared__ int s_last, s_ok[2];
     const uint32_t tid = threadIdx.x;
     if (tid == 0) {
         for (uint32_t i = 0; i < NS; ++i) {
             mbar_init(&full[i], 1);
-            mbar_init(&gath[i], 32);
-            mbar_init(&empty[i], kThreads / 32);
+            mbar_init(&meta[i], 1);
+            mbar_init(&gath[i], 64);
+            mbar_init(&empty[i], NC / 32);
         }
         fence_barrier_init();
     }
     __syncthreads();
-    if (tid >= kThreads) {
-        if (tid < kThreads + 32) spmv_producer<kMode>(sys, sp, smem, full, empty, desc, bdesc);
-        else if (tid < kThreads + 64) spmv_gatherer<kMode>(sys, sp, xplain, smem, full, gath, desc);
+    if (tid >= NC) {
+        if (tid < NC + 32) spmv_producer<kMode>(sys, sp, xplain, yplain, smem, full, meta, empty, desc, bdesc);
+        else spmv_gatherer<kMode>(sys, sp, xplain, smem, meta, gath, desc, (tid - NC - 32) >> 5);
         return;
     }
     uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles of run_sys published since the last ticket
-    uint32_t pend_sys = 0, pend_tile = 0;         // thread 0: tile whose warp partials wait in wred
-    bool pend = false;
+    double *pend_part = nullptr;                  // publisher: partial slot of the tile in wred
     for (uint32_t k = 0;; ++k) {
         const uint32_t s = k % NS, par = (k / NS) & 1u;
         // Thread 0 waits (bounded) and shares the outcome through a flag that
         // alternates with k, so a later write never meets an earlier read.
         if (tid == 0) s_ok[k & 1u] = (mbar_wait(&gath[s], par) && mbar_wait(&full[s], par)) ? 1 : 0;
-        csync();
+        csync<NC>();
         if (!s_ok[k & 1u]) {
             if (tid == 0) atomicOr(&sp->error, 1u);
             return;
         }
-        mbar_wait(&gath[s], par);  // completed: acquire in every thread
-        mbar_wait(&full[s], par);
-        const SpmvDesc d = desc[s];
+        mbar_observe(&gath[s], par);
+        mbar_observe(&full[s], par);
+        // The descriptor is read in place: it stays valid until this stage
+        // is handed back; what is needed after that is copied first.
+        const SpmvDesc &d = desc[s];
         // The previous tile's p.Ap partial: its warps' sums in warp order.
-        if (kMode == M_LOOP && tid == 0 && pend) {
-            const double *wr = wred + 8 * ((k - 1) & 1u);
+        if (kMode == M_LOOP && tid == kPublisher && pend_part) {
+            const double *wr = wred + (NC / 32) * ((k - 1) & 1u);
             double v = 0.0;
 #pragma unroll
-            for (int q = 0; q < kThreads / 32; ++q) v += wr[q];
-            sys[pend_sys].part_a[pend_tile] = v;
-            pend = false;
+            for (int q = 0; q < NC / 32; ++q) v += wr[q];
+            *pend_part = v;
+            pend_part = nullptr;
         }
         if (!d.valid) break;
         float *stage = smem + s * kSpmvStageFloats;
-        const SysDesc &S = sys[d.sys];
-        const float *__restrict__ xin = spmv_input<kMode>(S, xplain);
         if (kMode == M_LOOP && d.sys != run_sys) {
             flush_spmv(sys, run_sys, run_cnt, red, &s_last);
             run_sys = d.sys;
@@ -634,38 +724,42 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
         }
         const uint32_t row0 = d.layout == LAYOUT_BSR6 ? 6u * d.r0 : d.r0;
         const uint32_t nrows = d.layout == LAYOUT_BSR6 ? 6u * d.nr : d.nr;
+        const bool gathered = !d.lng && d.layout == LAYOUT_BSR6;
         float acc, p_own = 0.0f;
         bool own_ok = false;
-        if (!d.lng && d.layout == LAYOUT_BSR6) {
+        if (gathered) {
             acc = bsr_stage<kMode == M_LOOP>(d, stage, &p_own, &own_ok);
         } else {
             if (kMode == M_LOOP && tid < nrows) {
-                p_own = __ldg(xin + row0 + tid);
+                p_own = __ldg(d.x + row0 + tid);
                 own_ok = true;
             }
-            acc = d.lng ? long_tile(S, d, xin, stage) : csr_stage(d, xin, stage);
+            acc = d.lng ? long_tile(sys[d.sys], d, d.x, stage) : csr_stage(d, d.x, stage);
+            // These paths wrote into the stage: order those writes before the
+            // bulk copy that will next fill it.
+            fence_proxy_async();
         }
+        float *const yv = d.y;
+        const float *const xv = d.x;
+        double *const part_slot = d.part + d.tile;
         // Done reading the stage: hand it back to the producer.
-        fence_proxy_async();
         mbar_arrive_warp(&empty[s]);
         if (kMode == M_PLAIN) {
-            if (tid < nrows) yplain[row0 + tid] = acc;
+            if (tid < nrows) yv[row0 + tid] = acc;
         } else {
             double part = 0.0;
             if (tid < nrows) {
                 const uint32_t i = row0 + tid;
-                S.ap[i] = acc;
+                yv[i] = acc;
                 if (kMode == M_LOOP) {
-                    if (!own_ok) p_own = __ldg(xin + i);  // a block row without a diagonal block
+                    if (!own_ok) p_own = __ldg(xv + i);  // a block row without a diagonal block
                     part = (double)p_own * (double)acc;
                 }
             }
             if (kMode == M_LOOP) {
                 part = warp_sum(part);
-                if ((tid & 31u) == 0) wred[8 * (k & 1u) + (tid >> 5)] = part;
-                pend = true;
-                pend_sys = d.sys;
-                pend_tile = d.tile;
+                if ((tid & 31u) == 0) wred[(NC / 32) * (k & 1u) + (tid >> 5)] = part;
+                pend_part = part_slot;
                 ++run_cnt;
             }
         }
@@ -687,22 +781,33 @@ struct UpdDesc {
     uint32_t row0, rows, blk0, nblk;
     uint32_t ra, ba;  // 4-aligned starts of the staged row / block-start ranges
     float alpha;      // the system's alpha (loop kernel), read by the producer
-    uint32_t pad[2];
+    float *x, *r, *z, *p;
+    double2 *part;    // the system's per-tile (r.r, r.z) partials
+    const float *v0, *v1, *v2, *v3;  // bulk-copy sources of the staged vector slots (from ra)
+    const float *lu;                 // bulk-copy source of the tile's LU blocks
+    const uint32_t *bs;              // bulk-copy source of the tile's block starts (from ba)
 };
 
-// Resolves one work index of the update work list (one producer lane); false
+// Checks one work index of the update work list (one producer lane); false
 // past the end, for an invalid item (error code set) and, in the loop kernel,
 // for a system that is no longer active.
 template <bool kInit>
-__device__ __forceinline__ bool resolve_upd(const SysDesc *__restrict__ sys, const StepParams *sp, uint32_t idx,
-                                            uint32_t nw, WorkItem it, UpdDesc *d) {
+__device__ __forceinline__ bool check_upd(const SysDesc *__restrict__ sys, const StepParams *sp, uint32_t idx,
+                                          uint32_t nw, WorkItem it) {
     if (idx >= nw) return false;
     if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_utiles) {
         atomicOr(const_cast<uint32_t *>(&sp->error), 8u);  // invalid work item: skipped
         return false;
     }
-    if (!kInit && !sys[it.sys].st->active) return false;
-    const UpdTile T = sys[it.sys].utiles[it.tile];
+    return kInit || sys[it.sys].st->active;
+}
+
+// Fills the descriptor of a checked work item, field by field, in shared memory.
+template <bool kInit>
+__device__ __forceinline__ void fill_upd(const SysDesc *__restrict__ sys, WorkItem it, UpdDesc *d) {
+    const SysDesc &S = sys[it.sys];
+    const UpdTile T = S.utiles[it.tile];
+    const uint32_t ra = T.row0 & ~3u, ba = T.blk0 & ~3u;
     d->valid = 1;
     d->sys = it.sys;
     d->tile = it.tile;
@@ -710,33 +815,38 @@ __device__ __forceinline__ bool resolve_upd(const SysDesc *__restrict__ sys, con
     d->rows = T.row1 - T.row0;
     d->blk0 = T.blk0;
     d->nblk = T.blk1 - T.blk0;
-    d->ra = T.row0 & ~3u;
-    d->ba = T.blk0 & ~3u;
-    d->alpha = kInit ? 0.0f : sys[it.sys].st->alpha_f;
-    return true;
+    d->ra = ra;
+    d->ba = ba;
+    d->alpha = kInit ? 0.0f : S.st->alpha_f;
+    d->x = S.x;
+    d->r = S.r;
+    d->z = S.z;
+    d->p = S.p;
+    d->part = S.part_b;
+    d->v0 = (kInit ? S.b : S.x) + ra;
+    d->v1 = S.p + ra;
+    d->v2 = S.r + ra;
+    d->v3 = S.ap + ra;
+    d->lu = S.lu + (size_t)T.blk0 * 36u;
+    d->bs = S.bstart + ba;
 }
 
 // Stage slots: 0 = x (init: b), 1 = p, 2 = r, 3 = Ap; then LU and block starts.
 template <bool kInit>
-__device__ __forceinline__ void issue_upd(const SysDesc *__restrict__ sys, const UpdDesc &d, float *stage,
-                                          uint64_t *bar, uint64_t pol) {
-    const SysDesc &S = sys[d.sys];
+__device__ __forceinline__ void issue_upd(const UpdDesc &d, float *stage, uint64_t *bar, uint64_t pol) {
     const uint32_t vc = ((d.row0 + d.rows - d.ra) + 3) & ~3u;
     const uint32_t bc = ((d.blk0 + d.nblk + 1 - d.ba) + 3) & ~3u;
     const uint32_t lub = d.nblk * 144u;
     const uint32_t nvec = kInit ? 2u : 4u;
     mbar_expect_tx(bar, nvec * 4u * vc + lub + 4u * bc);
-    if (kInit) {
-        tma_load(stage, S.b + d.ra, 4u * vc, bar);
-        tma_load(stage + 3 * kVecCap, S.ap + d.ra, 4u * vc, bar);
-    } else {
-        tma_load(stage, S.x + d.ra, 4u * vc, bar);
-        tma_load(stage + kVecCap, S.p + d.ra, 4u * vc, bar);
-        tma_load(stage + 2 * kVecCap, S.r + d.ra, 4u * vc, bar);
-        tma_load(stage + 3 * kVecCap, S.ap + d.ra, 4u * vc, bar);
+    tma_load(stage, d.v0, 4u * vc, bar);
+    if (!kInit) {
+        tma_load(stage + kVecCap, d.v1, 4u * vc, bar);
+        tma_load(stage + 2 * kVecCap, d.v2, 4u * vc, bar);
     }
-    if (lub) tma_load_stream(stage + kLuOff, S.lu + (size_t)d.blk0 * 36u, lub, bar, pol);
-    tma_load_stream(stage + kBsOff, S.bstart + d.ba, 4u * bc, bar, pol);
+    tma_load(stage + 3 * kVecCap, d.v3, 4u * vc, bar);
+    if (lub) tma_load_stream(stage + kLuOff, d.lu, lub, bar, pol);
+    tma_load_stream(stage + kBsOff, d.bs, 4u * bc, bar, pol);
 }
 
 // The updated residual of row o of the stage (o relative to the staged
@@ -878,10 +988,9 @@ __device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, St
     bool err = false;
     const uint64_t pol = l2_evict_first_policy();
     for (;;) {
-        UpdDesc d;
-        const bool ok = resolve_upd<kInit>(sys, sp, base + lane * G, nw, it, &d);
+        const bool ok = check_upd<kInit>(sys, sp, base + lane * G, nw, it);
         const uint32_t m = __ballot_sync(0xffffffffu, ok);
-        if (ok) bdesc[__popc(m & ((1u << lane) - 1u))] = d;
+        if (ok) fill_upd<kInit>(sys, it, &bdesc[__popc(m & ((1u << lane) - 1u))]);
         const uint32_t cnt = __popc(m);
         base += 32u * G;
         const bool more = base < nw;
@@ -898,7 +1007,7 @@ __device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, St
                 }
                 if (i < cnt) {
                     desc[s] = bdesc[i];
-                    issue_upd<kInit>(sys, bdesc[i], smem + s * kUpdStageFloats, &full[s], pol);
+                    issue_upd<kInit>(desc[s], smem + s * kUpdStageFloats, &full[s], pol);
                     issued = k + 1;
                 } else {  // end marker
                     desc[s].valid = 0;
@@ -949,7 +1058,7 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
         return;
     }
     uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles of run_sys published since the last ticket
-    uint32_t pend_sys = 0, pend_tile = 0;         // thread 0: tile whose warp partials wait in wred
+    double2 *pend_part = nullptr;                 // thread 0: partial slot of the tile in wred
     bool pend = false;
     for (uint32_t k = 0;; ++k) {
         const uint32_t s = k % NS, par = (k / NS) & 1u;
@@ -959,8 +1068,10 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
             if (tid == 0) atomicOr(&sp->error, kInit ? 4u : 2u);
             return;
         }
-        mbar_wait(&full[s], par);  // completed: acquire in every thread
-        const UpdDesc d = desc[s];
+        mbar_observe(&full[s], par);
+        // The descriptor is read in place: it stays valid until this stage
+        // is handed back; what is needed after that is copied first.
+        const UpdDesc &d = desc[s];
         if (tid == 0 && pend) {
             const double2 *wr = wred + 8 * ((k - 1) & 1u);
             double va = 0.0, vb = 0.0;
@@ -969,7 +1080,7 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
                 va += wr[q].x;
                 vb += wr[q].y;
             }
-            sys[pend_sys].part_b[pend_tile] = make_double2(va, vb);
+            *pend_part = make_double2(va, vb);
             pend = false;
         }
         if (!d.valid) break;
@@ -978,7 +1089,6 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
             run_sys = d.sys;
             run_cnt = 0;
         }
-        const SysDesc &S = sys[d.sys];
         float *stage = smem + s * kUpdStageFloats;
         const uint32_t o = d.row0 - d.ra + tid;
         const float ma = -d.alpha;
@@ -992,36 +1102,39 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
                 da = (double)bi * (double)bi;
             } else {
                 const float xi = __fadd_rn(stage[o], __fmul_rn(d.alpha, stage[kVecCap + o]));
-                S.x[i] = xi;
+                d.x[i] = xi;
                 da = (double)ri * (double)ri;
             }
-            S.r[i] = ri;
+            d.r[i] = ri;
         }
         const uint32_t tag = k + 1;
         bj_stage<kInit>(d, stage, sz, sflag, tag);
-        // Every thread is done with the stage: hand it back to the producer.
-        fence_proxy_async();
+        const uint32_t rows = d.rows, row0 = d.row0;
+        float *const zv = d.z;
+        float *const pv = d.p;
+        double2 *const part_slot = d.part + d.tile;
+        // Every thread is done reading the stage (it wrote nothing into it):
+        // hand it back to the producer.
         mbar_arrive_warp(&empty[s]);
         csync();
         double rz = 0.0;
-        if (tid < d.rows) {
-            const uint32_t i = d.row0 + tid;
+        if (tid < rows) {
+            const uint32_t i = row0 + tid;
             float zi;
             if (sflag[tid] == tag) {
                 zi = sz[tid];
-                S.z[i] = zi;
+                zv[i] = zi;
             } else {
-                zi = S.z[i];  // a row the block solve leaves alone (position >= 6 in its block)
+                zi = zv[i];  // a row the block solve leaves alone (position >= 6 in its block)
             }
-            if (kInit) S.p[i] = zi;
+            if (kInit) pv[i] = zi;
             rz = (double)ri * (double)zi;
         }
         da = warp_sum(da);
         rz = warp_sum(rz);
         if ((tid & 31u) == 0) wred[8 * (k & 1u) + (tid >> 5)] = make_double2(da, rz);
         pend = true;
-        pend_sys = d.sys;
-        pend_tile = d.tile;
+        pend_part = part_slot;
         ++run_cnt;
     }
     if (run_sys != 0xffffffffu) flush_upd<kInit>(sys, sp, run_sys, run_cnt, red, &s_last);
@@ -1029,17 +1142,17 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
 
 }  // namespace
 
-__global__ void __launch_bounds__(kSpmvThreads, 3) k_spmv_loop(const SysDesc *__restrict__ sys, StepParams *sp) {
+__global__ void __launch_bounds__(kSpmvThreads, kSpmvMinCtas) k_spmv_loop(const SysDesc *__restrict__ sys, StepParams *sp) {
     extern __shared__ __align__(128) float smem[];
     spmv_pipeline<M_LOOP>(sys, sp, nullptr, nullptr, smem);
 }
 
-__global__ void __launch_bounds__(kSpmvThreads, 3) k_spmv_init(const SysDesc *__restrict__ sys, StepParams *sp) {
+__global__ void __launch_bounds__(kSpmvThreads, kSpmvMinCtas) k_spmv_init(const SysDesc *__restrict__ sys, StepParams *sp) {
     extern __shared__ __align__(128) float smem[];
     spmv_pipeline<M_INIT>(sys, sp, nullptr, nullptr, smem);
 }
 
-__global__ void __launch_bounds__(kSpmvThreads, 3) k_spmv_plain(const SysDesc *__restrict__ sys, StepParams *sp,
+__global__ void __launch_bounds__(kSpmvThreads, kSpmvMinCtas) k_spmv_plain(const SysDesc *__restrict__ sys, StepParams *sp,
                                                          const float *__restrict__ x, float *__restrict__ y) {
     extern __shared__ __align__(128) float smem[];
     spmv_pipeline<M_PLAIN>(sys, sp, x, y, smem);

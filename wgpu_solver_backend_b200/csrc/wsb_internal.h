@@ -23,10 +23,10 @@ namespace wsb {
 // (-DWSB_CSR_CAP=..., -DWSB_BSR_CAP=..., -DWSB_SPMV_STAGES=...) for tuning
 // sweeps; the host tiling and the kernels always use the same values.
 #ifndef WSB_CSR_CAP
-#define WSB_CSR_CAP 4096
+#define WSB_CSR_CAP 2048
 #endif
 #ifndef WSB_BSR_CAP
-#define WSB_BSR_CAP 192
+#define WSB_BSR_CAP 128
 #endif
 #ifndef WSB_SPMV_STAGES
 #define WSB_SPMV_STAGES 2
@@ -34,8 +34,13 @@ namespace wsb {
 #ifndef WSB_UPD_STAGES
 #define WSB_UPD_STAGES 3
 #endif
-constexpr int kThreads = 256;        // threads per CTA for every solver kernel
-constexpr int kTileRows = 256;       // rows (or block rows x 6) per tile, <= kThreads
+#ifndef WSB_SPMV_CONSUMERS
+#define WSB_SPMV_CONSUMERS 128
+#endif
+constexpr int kThreads = 256;        // consumer threads per CTA of the update and vector kernels
+constexpr int kTileRows = 256;       // rows per update tile, <= kThreads
+constexpr int kSpmvConsumers = WSB_SPMV_CONSUMERS;  // consumer threads per CTA of the SpMV kernels
+constexpr int kSpmvTileRows = kSpmvConsumers;       // rows (or block rows x 6) per SpMV tile
 constexpr int kCsrCap = WSB_CSR_CAP;         // CSR nonzeros per SpMV tile (one TMA stage)
 constexpr int kBsrCapBlocks = WSB_BSR_CAP;   // BSR 6x6 blocks per SpMV tile (144 B each)
 constexpr int kSpmvStages = WSB_SPMV_STAGES; // depth of the SpMV shared-memory ring
