@@ -140,7 +140,7 @@ Engine::Engine(Context *ctx, cudaStream_t stream) : ctx_(ctx), stream_(stream) {
     cudaFuncSetAttribute(k_init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdSmem);
     int occ_a = 0, occ_b = 0, occ_c = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_spmv_loop, kSpmvThreads, kSpmvSmem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_update, kPipeThreads, kUpdSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_update, kUpdThreads, kUpdSmem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_pupdate, kThreads, 0);
     max_grid_a_ = std::max(1, occ_a) * std::max(1, ctx->sm_count);
     max_grid_b_ = std::max(1, occ_b) * std::max(1, ctx->sm_count);
@@ -446,7 +446,7 @@ int Engine::capture_loop(uint32_t ga, uint32_t gb, uint32_t gc) {
     cudaError_t e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
     if (e == cudaSuccess) {
         k_spmv_loop<<<ga, kSpmvThreads, kSpmvSmem, cs>>>(d_sys_, d_sp_);
-        k_update<<<gb, kPipeThreads, kUpdSmem, cs>>>(d_sys_, d_sp_);
+        k_update<<<gb, kUpdThreads, kUpdSmem, cs>>>(d_sys_, d_sp_);
         k_pupdate<<<gc, kThreads, 0, cs>>>(d_sys_, d_sp_, h);
         e = cudaStreamEndCapture(cs, &body);
     }
@@ -625,7 +625,7 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
         const uint32_t ga = std::min<uint32_t>(h_sp_->n_init_a, (uint32_t)max_grid_a_);
         const uint32_t gb = std::min<uint32_t>(h_sp_->n_init_b, (uint32_t)max_grid_b_);
         if (ga) k_spmv_init<<<ga, kSpmvThreads, kSpmvSmem, stream_>>>(d_sys_, d_sp_);
-        if (gb) k_init<<<gb, kPipeThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
+        if (gb) k_init<<<gb, kUpdThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
         WSB_CUDA_TRY(ctx_, cudaGetLastError());
         launches_ += (ga ? 1 : 0) + (gb ? 1 : 0);
     }
@@ -645,7 +645,7 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
                 const uint32_t burst = std::min<uint32_t>(16, limit - done_iters);
                 for (uint32_t i = 0; i < burst; ++i) {
                     k_spmv_loop<<<ga, kSpmvThreads, kSpmvSmem, stream_>>>(d_sys_, d_sp_);
-                    k_update<<<gb, kPipeThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
+                    k_update<<<gb, kUpdThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
                     k_pupdate<<<gc, kThreads, 0, stream_>>>(d_sys_, d_sp_, 0);
                 }
                 WSB_CUDA_TRY(ctx_, cudaGetLastError());
@@ -746,14 +746,14 @@ int Engine::profile_kernels(uint32_t s, uint32_t iters, double ms[5]) {
     const uint32_t gb = std::min<uint32_t>(n_work_b_, (uint32_t)max_grid_b_);
     const uint32_t gc = std::min<uint32_t>(n_work_c_, (uint32_t)max_grid_c_);
     k_spmv_init<<<std::min<uint32_t>(h_sp_->n_init_a, (uint32_t)max_grid_a_), kSpmvThreads, kSpmvSmem, stream_>>>(d_sys_, d_sp_);
-    k_init<<<std::min<uint32_t>(h_sp_->n_init_b, (uint32_t)max_grid_b_), kPipeThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
+    k_init<<<std::min<uint32_t>(h_sp_->n_init_b, (uint32_t)max_grid_b_), kUpdThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
     std::vector<cudaEvent_t> ev(4 * (size_t)iters);
     for (auto &e : ev) WSB_CUDA_TRY(ctx_, cudaEventCreate(&e));
     for (uint32_t i = 0; i < iters; ++i) {
         cudaEventRecord(ev[4 * i + 0], stream_);
         k_spmv_loop<<<ga, kSpmvThreads, kSpmvSmem, stream_>>>(d_sys_, d_sp_);
         cudaEventRecord(ev[4 * i + 1], stream_);
-        k_update<<<gb, kPipeThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
+        k_update<<<gb, kUpdThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
         cudaEventRecord(ev[4 * i + 2], stream_);
         k_pupdate<<<gc, kThreads, 0, stream_>>>(d_sys_, d_sp_, 0);
         cudaEventRecord(ev[4 * i + 3], stream_);

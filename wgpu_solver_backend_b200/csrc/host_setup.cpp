@@ -214,7 +214,7 @@ void build_spmv_tiles_bsr(uint32_t nbrows, const uint32_t *brow_ptr, std::vector
     }
 }
 
-// Update tiles of <= kTileRows rows holding <= kUpdBlocks block starts. A cut
+// Update tiles of <= kUpdTileRows rows holding <= kUpdBlocks block starts. A cut
 // is allowed at a block start or at a row whose position inside its block is
 // >= 6 (the reference never touches z there, block_jacobi.wgsl:79,124-126),
 // so the solved rows of a block are always inside one tile.
@@ -237,7 +237,7 @@ void build_upd_tiles(uint32_t n, const uint32_t *bs, uint32_t nb, std::vector<Up
     }
     uint32_t r0 = 0;
     while (r0 < n) {
-        uint32_t r1 = std::min<uint32_t>(n, r0 + kTileRows);
+        uint32_t r1 = std::min<uint32_t>(n, r0 + kUpdTileRows);
         while (r1 > r0 + 1 && (!cut_ok[r1] || starts_before[r1] - starts_before[r0] > (uint32_t)kUpdBlocks)) --r1;
         // r0 + 1 is always a cut when the block at r0 has one row or r0 is a
         // passive row; otherwise the loop stops at the next block start.

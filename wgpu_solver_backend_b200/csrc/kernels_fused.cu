@@ -770,7 +770,8 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
 // ---------------------------------------------------------------------------
 // Update tiles (x, r, z and the block-Jacobi solve)
 // ---------------------------------------------------------------------------
-constexpr int kVecCap = kTileRows + 8;                    // floats per staged vector slice
+constexpr int NU = kUpdConsumers;                         // consumer threads of the update kernels
+constexpr int kVecCap = kUpdTileRows + 8;                 // floats per staged vector slice
 constexpr int kLuOff = 4 * kVecCap;                       // LU blocks
 constexpr int kBsOff = kLuOff + kUpdBlocks * 36;          // block starts slice
 static_assert((kLuOff * 4) % 16 == 0 && (kBsOff * 4) % 16 == 0 && (kVecCap * 4) % 16 == 0, "TMA alignment");
@@ -923,8 +924,8 @@ __device__ __forceinline__ void flush_upd(const SysDesc *__restrict__ sys, StepP
     if (cnt == 0) return;
     const SysDesc &S = sys[s];
     SysState *st = S.st;
-    if (!take_ticket(&st->cnt_b, cnt, S.n_utiles, s_last)) return;
-    const double2 sum = sum_partials2(S.part_b, S.n_utiles, red);
+    if (!take_ticket<NU>(&st->cnt_b, cnt, S.n_utiles, s_last)) return;
+    const double2 sum = sum_partials2<NU>(S.part_b, S.n_utiles, red);
     if (threadIdx.x != 0) return;
     if (kInit) {
         st->bb = sum.x;
@@ -1038,23 +1039,23 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
     __shared__ __align__(8) uint64_t full[NS], empty[NS];
     __shared__ UpdDesc desc[NS];
     __shared__ UpdDesc bdesc[32];
-    __shared__ float sz[kTileRows];
-    __shared__ uint32_t sflag[kTileRows];
+    __shared__ float sz[kUpdTileRows];
+    __shared__ uint32_t sflag[kUpdTileRows];
     __shared__ double red[64];
-    __shared__ double2 wred[2 * (kThreads / 32)];
+    __shared__ double2 wred[2 * (NU / 32)];
     __shared__ int s_last, s_ok[2];
     const uint32_t tid = threadIdx.x;
     if (tid == 0) {
         for (uint32_t i = 0; i < NS; ++i) {
             mbar_init(&full[i], 1);
-            mbar_init(&empty[i], kThreads / 32);
+            mbar_init(&empty[i], NU / 32);
         }
         fence_barrier_init();
     }
-    if (tid < kTileRows) sflag[tid] = 0u;
+    if (tid < kUpdTileRows) sflag[tid] = 0u;
     __syncthreads();
-    if (tid >= kThreads) {
-        if (tid < kThreads + 32) upd_producer<kInit>(sys, sp, smem, full, empty, desc, bdesc);
+    if (tid >= NU) {
+        if (tid < NU + 32) upd_producer<kInit>(sys, sp, smem, full, empty, desc, bdesc);
         return;
     }
     uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles of run_sys published since the last ticket
@@ -1063,7 +1064,7 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
     for (uint32_t k = 0;; ++k) {
         const uint32_t s = k % NS, par = (k / NS) & 1u;
         if (tid == 0) s_ok[k & 1u] = mbar_wait(&full[s], par) ? 1 : 0;
-        csync();
+        csync<NU>();
         if (!s_ok[k & 1u]) {
             if (tid == 0) atomicOr(&sp->error, kInit ? 4u : 2u);
             return;
@@ -1073,10 +1074,10 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
         // is handed back; what is needed after that is copied first.
         const UpdDesc &d = desc[s];
         if (tid == 0 && pend) {
-            const double2 *wr = wred + 8 * ((k - 1) & 1u);
+            const double2 *wr = wred + (NU / 32) * ((k - 1) & 1u);
             double va = 0.0, vb = 0.0;
 #pragma unroll
-            for (int q = 0; q < kThreads / 32; ++q) {
+            for (int q = 0; q < NU / 32; ++q) {
                 va += wr[q].x;
                 vb += wr[q].y;
             }
@@ -1116,7 +1117,7 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
         // Every thread is done reading the stage (it wrote nothing into it):
         // hand it back to the producer.
         mbar_arrive_warp(&empty[s]);
-        csync();
+        csync<NU>();
         double rz = 0.0;
         if (tid < rows) {
             const uint32_t i = row0 + tid;
@@ -1132,7 +1133,7 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
         }
         da = warp_sum(da);
         rz = warp_sum(rz);
-        if ((tid & 31u) == 0) wred[8 * (k & 1u) + (tid >> 5)] = make_double2(da, rz);
+        if ((tid & 31u) == 0) wred[(NU / 32) * (k & 1u) + (tid >> 5)] = make_double2(da, rz);
         pend = true;
         pend_part = part_slot;
         ++run_cnt;
@@ -1158,12 +1159,12 @@ __global__ void __launch_bounds__(kSpmvThreads, kSpmvMinCtas) k_spmv_plain(const
     spmv_pipeline<M_PLAIN>(sys, sp, x, y, smem);
 }
 
-__global__ void __launch_bounds__(kPipeThreads, 4) k_update(const SysDesc *__restrict__ sys, StepParams *sp) {
+__global__ void __launch_bounds__(kUpdThreads, kUpdMinCtas) k_update(const SysDesc *__restrict__ sys, StepParams *sp) {
     extern __shared__ __align__(128) float smem[];
     upd_pipeline<false>(sys, sp, smem);
 }
 
-__global__ void __launch_bounds__(kPipeThreads, 4) k_init(const SysDesc *__restrict__ sys, StepParams *sp) {
+__global__ void __launch_bounds__(kUpdThreads, kUpdMinCtas) k_init(const SysDesc *__restrict__ sys, StepParams *sp) {
     extern __shared__ __align__(128) float smem[];
     upd_pipeline<true>(sys, sp, smem);
 }

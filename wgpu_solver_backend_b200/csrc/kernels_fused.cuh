@@ -28,15 +28,19 @@ constexpr int kSpmvBsrEnd = kSpmvXgOff + 6 * kBsrCapBlocks;
 constexpr int kSpmvCsrEnd = 2 * (kCsrCap + 8);
 constexpr int kSpmvRpOff = (((kSpmvCsrEnd > kSpmvBsrEnd) ? kSpmvCsrEnd : kSpmvBsrEnd) + 3) & ~3;
 constexpr int kSpmvStageFloats = ((kSpmvRpOff + kSpmvTileRows + 8) + 31) & ~31;
-constexpr int kUpdStageFloats = ((4 * (kTileRows + 8) + kUpdBlocks * 36 + kUpdBlocks + 8) + 31) & ~31;
-// Threads per CTA of the TMA-pipelined kernels: consumers (kThreads in the
-// update kernels, kSpmvConsumers in the SpMV) plus one producer warp, plus
-// the gather warps in the SpMV.
+constexpr int kUpdStageFloats = ((4 * (kUpdTileRows + 8) + kUpdBlocks * 36 + kUpdBlocks + 8) + 31) & ~31;
+// Threads per CTA of the TMA-pipelined kernels: consumers (kUpdConsumers in
+// the update kernels, kSpmvConsumers in the SpMV) plus one producer warp,
+// plus the gather warps in the SpMV.
 #ifndef WSB_GATHER_WARPS
 #define WSB_GATHER_WARPS 1
 #endif
 constexpr int kGatherWarps = WSB_GATHER_WARPS;
-constexpr int kPipeThreads = kThreads + 32;
+constexpr int kUpdThreads = kUpdConsumers + 32;
+#ifndef WSB_UPD_MIN_CTAS
+#define WSB_UPD_MIN_CTAS 4
+#endif
+constexpr int kUpdMinCtas = WSB_UPD_MIN_CTAS;
 constexpr int kSpmvThreads = kSpmvConsumers + 32 + 32 * kGatherWarps;
 // CTAs per SM the SpMV kernels are compiled for (register budget).
 #ifndef WSB_SPMV_MIN_CTAS

@@ -37,14 +37,21 @@ namespace wsb {
 #ifndef WSB_SPMV_CONSUMERS
 #define WSB_SPMV_CONSUMERS 128
 #endif
-constexpr int kThreads = 256;        // consumer threads per CTA of the update and vector kernels
-constexpr int kTileRows = 256;       // rows per update tile, <= kThreads
+#ifndef WSB_UPD_CONSUMERS
+#define WSB_UPD_CONSUMERS 256
+#endif
+#ifndef WSB_UPD_BLOCKS
+#define WSB_UPD_BLOCKS 64
+#endif
+constexpr int kThreads = 256;        // threads per CTA of the vector and refinement kernels
+constexpr int kUpdConsumers = WSB_UPD_CONSUMERS;   // consumer threads per CTA of the update kernels
+constexpr int kUpdTileRows = kUpdConsumers;        // rows per update tile (<= kThreads)
 constexpr int kSpmvConsumers = WSB_SPMV_CONSUMERS;  // consumer threads per CTA of the SpMV kernels
 constexpr int kSpmvTileRows = kSpmvConsumers;       // rows (or block rows x 6) per SpMV tile
 constexpr int kCsrCap = WSB_CSR_CAP;         // CSR nonzeros per SpMV tile (one TMA stage)
 constexpr int kBsrCapBlocks = WSB_BSR_CAP;   // BSR 6x6 blocks per SpMV tile (144 B each)
 constexpr int kSpmvStages = WSB_SPMV_STAGES; // depth of the SpMV shared-memory ring
-constexpr int kUpdBlocks = 64;       // block-Jacobi blocks per update tile
+constexpr int kUpdBlocks = WSB_UPD_BLOCKS;         // block-Jacobi blocks per update tile
 constexpr int kUpdStages = WSB_UPD_STAGES;   // depth of the update shared-memory ring
 static_assert(kCsrCap % 4 == 0 && kBsrCapBlocks % 4 == 0 && kSpmvStages >= 2, "SpMV tile caps");
 constexpr int kChunkRows = 4096;     // rows per work item of the vector kernels
