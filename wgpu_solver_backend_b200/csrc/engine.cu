@@ -12,6 +12,25 @@ namespace wsb {
 
 static inline size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Launch with programmatic stream serialisation: the kernel may begin while
+// the previous kernel in the stream drains; it waits for that kernel's
+// completion itself (griddepcontrol.wait) before touching its results.
+template <typename... Params, typename... Args>
+static cudaError_t launch_pdl(void (*kernel)(Params...), uint32_t grid, uint32_t block, size_t smem,
+                              cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 MatA::~MatA() {
     dev_free(row_ptr);
     dev_free(col);
@@ -445,10 +464,13 @@ int Engine::capture_loop(uint32_t ga, uint32_t gb, uint32_t gc) {
     WSB_CUDA_TRY(ctx_, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaError_t e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
     if (e == cudaSuccess) {
-        k_spmv_loop<<<ga, kSpmvThreads, kSpmvSmem, cs>>>(d_sys_, d_sp_);
-        k_update<<<gb, kUpdThreads, kUpdSmem, cs>>>(d_sys_, d_sp_);
-        k_pupdate<<<gc, kThreads, 0, cs>>>(d_sys_, d_sp_, h);
+        const SysDesc *dsys = d_sys_;
+        StepParams *dsp = d_sp_;
+        cudaError_t le = launch_pdl(k_spmv_loop, ga, kSpmvThreads, kSpmvSmem, cs, dsys, dsp);
+        if (le == cudaSuccess) le = launch_pdl(k_update, gb, kUpdThreads, kUpdSmem, cs, dsys, dsp);
+        if (le == cudaSuccess) le = launch_pdl(k_pupdate, gc, kThreads, (size_t)0, cs, dsys, dsp, h);
         e = cudaStreamEndCapture(cs, &body);
+        if (e == cudaSuccess && le != cudaSuccess) e = le;
     }
     cudaStreamDestroy(cs);
     if (e != cudaSuccess) return fail(ctx_, WSB_ERR_CUDA, "capturing the PCG loop body failed: %s", cudaGetErrorString(e));
@@ -624,9 +646,10 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
     if (!init.empty()) {
         const uint32_t ga = std::min<uint32_t>(h_sp_->n_init_a, (uint32_t)max_grid_a_);
         const uint32_t gb = std::min<uint32_t>(h_sp_->n_init_b, (uint32_t)max_grid_b_);
-        if (ga) k_spmv_init<<<ga, kSpmvThreads, kSpmvSmem, stream_>>>(d_sys_, d_sp_);
-        if (gb) k_init<<<gb, kUpdThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
-        WSB_CUDA_TRY(ctx_, cudaGetLastError());
+        const SysDesc *dsys = d_sys_;
+        StepParams *dsp = d_sp_;
+        if (ga) WSB_CUDA_TRY(ctx_, launch_pdl(k_spmv_init, ga, kSpmvThreads, kSpmvSmem, stream_, dsys, dsp));
+        if (gb) WSB_CUDA_TRY(ctx_, launch_pdl(k_init, gb, kUpdThreads, kUpdSmem, stream_, dsys, dsp));
         launches_ += (ga ? 1 : 0) + (gb ? 1 : 0);
     }
     if (num_active_ > 0 && n_work_a_ > 0) {
@@ -643,10 +666,13 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
             uint32_t done_iters = 0;
             while (done_iters < limit) {
                 const uint32_t burst = std::min<uint32_t>(16, limit - done_iters);
+                const SysDesc *dsys = d_sys_;
+                StepParams *dsp = d_sp_;
+                const cudaGraphConditionalHandle none = 0;
                 for (uint32_t i = 0; i < burst; ++i) {
-                    k_spmv_loop<<<ga, kSpmvThreads, kSpmvSmem, stream_>>>(d_sys_, d_sp_);
-                    k_update<<<gb, kUpdThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
-                    k_pupdate<<<gc, kThreads, 0, stream_>>>(d_sys_, d_sp_, 0);
+                    WSB_CUDA_TRY(ctx_, launch_pdl(k_spmv_loop, ga, kSpmvThreads, kSpmvSmem, stream_, dsys, dsp));
+                    WSB_CUDA_TRY(ctx_, launch_pdl(k_update, gb, kUpdThreads, kUpdSmem, stream_, dsys, dsp));
+                    WSB_CUDA_TRY(ctx_, launch_pdl(k_pupdate, gc, kThreads, (size_t)0, stream_, dsys, dsp, none));
                 }
                 WSB_CUDA_TRY(ctx_, cudaGetLastError());
                 done_iters += burst;

@@ -129,6 +129,15 @@ __device__ __forceinline__ void mbar_observe(uint64_t *bar, uint32_t parity) {
     if (!mbar_test_wait(bar, parity)) mbar_wait(bar, parity);
 }
 
+// Programmatic dependent launch: the next kernel in the stream may start
+// launching its CTAs now (they occupy SMs only as this kernel's CTAs leave);
+// and this kernel waits until the previous one has completed and its memory
+// is visible. Both are no-ops for a launch without the attribute.
+__device__ __forceinline__ void pdl_start() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -684,6 +693,7 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
         fence_barrier_init();
     }
     __syncthreads();
+    pdl_start();
     if (tid >= NC) {
         if (tid < NC + 32) spmv_producer<kMode>(sys, sp, xplain, yplain, smem, full, meta, empty, desc, bdesc);
         else spmv_gatherer<kMode>(sys, sp, xplain, smem, meta, gath, desc, (tid - NC - 32) >> 5);
@@ -1054,6 +1064,7 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
     }
     if (tid < kUpdTileRows) sflag[tid] = 0u;
     __syncthreads();
+    pdl_start();
     if (tid >= NU) {
         if (tid < NU + 32) upd_producer<kInit>(sys, sp, smem, full, empty, desc, bdesc);
         return;
@@ -1177,6 +1188,7 @@ __global__ void __launch_bounds__(kUpdThreads, kUpdMinCtas) k_init(const SysDesc
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kThreads) k_pupdate(const SysDesc *__restrict__ sys, StepParams *sp,
                                                       cudaGraphConditionalHandle h) {
+    pdl_start();
     const uint32_t nw = sp->n_work_c;
     const WorkItem *__restrict__ work = sp->work_c;
     for (uint32_t w = blockIdx.x; w < nw; w += gridDim.x) {
@@ -1234,6 +1246,7 @@ __global__ void __launch_bounds__(kThreads) k_pupdate(const SysDesc *__restrict_
 // Parent-graph node in front of the while loop: resets the step's iteration
 // count and skips the loop when nothing is active.
 __global__ void k_loop_gate(StepParams *sp, cudaGraphConditionalHandle h) {
+    pdl_start();
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         sp->loop_count = 0;
         cudaGraphSetConditional(h, (sp->num_active > 0 && sp->loop_limit > 0 && sp->error == 0) ? 1u : 0u);
