@@ -251,6 +251,11 @@ int wsb_matrix_create(wsb_context *ctx, uint32_t n, const uint32_t *row_ptr, con
                       uint64_t block_starts_len, int32_t layout, wsb_matrix **out);
 int wsb_matrix_info_get(const wsb_matrix *m, wsb_matrix_info *out);
 void wsb_matrix_destroy(wsb_matrix *m);
+/* Copies the block-Jacobi factors the handle holds (built on the device,   */
+/* num_blocks * 36 floats, the layout and bits of the Vec<f32> that         */
+/* build_lu_blocks_from_csr_block_starts_6 returns, compute.rs:84-181)      */
+/* into out; out_len must be at least num_blocks * 36.                      */
+int wsb_matrix_read_lu(wsb_context *ctx, const wsb_matrix *m, float *out, uint64_t out_len);
 
 /* Solve A x = b with host arrays (copies inside the call). */
 int wsb_solve(wsb_context *ctx, wsb_matrix *m, const float *b, float *x, uint64_t max_iter, float rel_tol,

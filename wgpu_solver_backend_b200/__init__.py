@@ -374,6 +374,14 @@ class Matrix:
                                                C.byref(h)), ctx.handle)
         return Matrix(ctx, h)
 
+    def lu(self) -> np.ndarray:
+        """The block-Jacobi factors held on the device (num_blocks * 36
+        floats, the layout of build_lu_blocks_from_csr_block_starts_6)."""
+        out = np.zeros(max(1, int(self.info["num_blocks"]) * 36), np.float32)
+        _check(_lib_handle().wsb_matrix_read_lu(self.ctx.handle, self.handle, _p(out, _lib.f32p), out.size),
+               self.ctx.handle)
+        return out[: int(self.info["num_blocks"]) * 36]
+
     def solve(self, b, x0=None, max_iter=2000, rel_tol=1e-8, abs_tol=0.0, precision=PREC_F32_F64DOT,
               history_capacity=0, always_write_x=False, raise_on_error=True, **mixed):
         """Returns (x, result dict). x keeps x0 unless the solve succeeded (or

@@ -105,6 +105,7 @@ SIGNATURES = {
                                     C.POINTER(vp)]),
     "wsb_matrix_info_get": (C.c_int, [vp, C.POINTER(MatrixInfo)]),
     "wsb_matrix_destroy": (None, [vp]),
+    "wsb_matrix_read_lu": (C.c_int, [vp, vp, f32p, C.c_uint64]),
     "wsb_solve": (C.c_int, [vp, vp, f32p, f32p, C.c_uint64, C.c_float, C.c_float, C.POINTER(SolveOpts),
                             C.POINTER(SolveResult)]),
     "wsb_solve_device": (C.c_int, [vp, vp, vp, vp, C.c_uint64, C.c_float, C.c_float, C.POINTER(SolveOpts),

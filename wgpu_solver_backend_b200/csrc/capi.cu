@@ -716,16 +716,10 @@ extern "C" int wsb_matrix_create(wsb_context *ctx, uint32_t n, const uint32_t *r
     if (!out) return fail(ctx, WSB_ERR_BAD_INPUT, "out is null");
     *out = nullptr;
     if (nnz > 0xfffff000ull) return fail(ctx, WSB_ERR_BAD_INPUT, "nnz %llu exceeds the u32 index range", (unsigned long long)nnz);
-    std::string err;
-    int rc = validate_system(n, row_ptr, col, nnz, bs, bs_len, &err);
-    if (rc) return fail(ctx, rc, "%s", err.c_str());
-    std::vector<float> lu((bs_len - 1) * 36 + 1);
-    rc = build_lu_blocks_6(n, row_ptr, (uint64_t)n + 1, col, nnz, val, nnz, bs, bs_len, lu.data(), &err);
-    if (rc) return fail(ctx, rc, "%s", err.c_str());
+    if (!row_ptr || (nnz && (!col || !val))) return fail(ctx, WSB_ERR_BAD_INPUT, "null CSR array");
     auto *m = new wsb_matrix();
     m->ctx = ctx;
-    rc = upload_matA(ctx, n, row_ptr, col, val, nnz, bs, bs_len, layout, ctx->stream, &m->A);
-    if (!rc) rc = upload_precond(ctx, n, lu.data(), bs, bs_len, ctx->stream, &m->M);
+    int rc = prepare_system_device(ctx, n, row_ptr, col, val, nnz, bs, bs_len, layout, ctx->stream, &m->A, &m->M);
     if (rc) {
         delete m;
         return rc;
@@ -744,6 +738,19 @@ extern "C" int wsb_matrix_info_get(const wsb_matrix *m, wsb_matrix_info *out) {
     out->device_bytes = m->A.bytes + m->M.bytes;
     out->spmv_bytes = spmv_algorithmic_bytes(m->A);
     out->iteration_bytes = iteration_algorithmic_bytes(m->A, m->M);
+    return WSB_OK;
+}
+
+extern "C" int wsb_matrix_read_lu(wsb_context *ctx, const wsb_matrix *m, float *out, uint64_t out_len) {
+    CHECK_CTX(ctx);
+    if (!m || (!out && m->M.nb)) return fail(ctx, WSB_ERR_BAD_INPUT, "bad arguments");
+    const uint64_t need = 36ull * m->M.nb;
+    if (out_len < need) return fail(ctx, WSB_ERR_BAD_INPUT, "out_len %llu < %llu", (unsigned long long)out_len,
+                                    (unsigned long long)need);
+    if (need) {
+        WSB_CUDA_TRY(ctx, cudaMemcpyAsync(out, m->M.lu, sizeof(float) * need, cudaMemcpyDeviceToHost, ctx->stream));
+        WSB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    }
     return WSB_OK;
 }
 

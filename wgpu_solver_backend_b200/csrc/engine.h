@@ -43,6 +43,13 @@ int upload_matA(Context *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_
                 uint64_t nnz, const uint32_t *bs, uint64_t bs_len, int layout_req, cudaStream_t st, MatA *out);
 int upload_precond(Context *ctx, uint32_t n, const float *lu, const uint32_t *bs, uint64_t bs_len,
                    cudaStream_t st, Precond *out);
+// Uploads a system's CSR arrays and block starts and prepares the rest on the
+// device (column check, BSR6 test and conversion, block-Jacobi LU); host
+// work is limited to O(n) checks and the tile lists. Status and message as
+// the host path (validate_system, build_lu_blocks_6, upload_matA).
+int prepare_system_device(Context *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_t *col, const float *val,
+                          uint64_t nnz, const uint32_t *bs, uint64_t bs_len, int layout_req, cudaStream_t st,
+                          MatA *A, Precond *M);
 uint64_t spmv_algorithmic_bytes(const MatA &A);
 uint64_t iteration_algorithmic_bytes(const MatA &A, const Precond &M);
 

@@ -128,7 +128,7 @@ int build_lu_blocks_6(uint32_t n, const uint32_t *row_ptr, uint64_t row_ptr_len,
 // Matrix and partition checks of loaders.rs:83-113 and loaders.rs:164-184,
 // plus the bounds every kernel relies on.
 int validate_system(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, uint64_t nnz,
-                    const uint32_t *bs, uint64_t bs_len, std::string *err) {
+                    const uint32_t *bs, uint64_t bs_len, std::string *err, bool check_cols) {
     if (!row_ptr) {
         *err = "row_ptr is null";
         return WSB_ERR_BAD_INPUT;
@@ -151,8 +151,9 @@ int validate_system(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, ui
         return WSB_ERR_BAD_INPUT;
     }
     uint32_t max_col = 0;
-    for (uint64_t k = 0; k < nnz; ++k) max_col = std::max(max_col, col[k]);
-    if (nnz && max_col >= n) {
+    if (check_cols)
+        for (uint64_t k = 0; k < nnz; ++k) max_col = std::max(max_col, col[k]);
+    if (check_cols && nnz && max_col >= n) {
         *err = fmt("CSR col_idx contains out-of-range column %u for n_cols=%u", max_col, n);
         return WSB_ERR_BAD_INPUT;
     }

@@ -192,8 +192,10 @@ int build_lu_blocks_6(uint32_t n, const uint32_t *row_ptr, uint64_t row_ptr_len,
                       uint64_t col_len, const float *val, uint64_t val_len, const uint32_t *bs,
                       uint64_t bs_len, float *out, std::string *err);
 // Validation of a CSR matrix + block partition (loaders.rs:44-212 rules).
+// With check_cols false the O(nnz) column-range scan is left to the caller
+// (the device-side preparation does it on the GPU).
 int validate_system(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, uint64_t nnz,
-                    const uint32_t *bs, uint64_t bs_len, std::string *err);
+                    const uint32_t *bs, uint64_t bs_len, std::string *err, bool check_cols = true);
 
 void build_spmv_tiles_csr(uint32_t n, const uint32_t *row_ptr, std::vector<SpmvTile> *out);
 void build_spmv_tiles_bsr(uint32_t nbrows, const uint32_t *brow_ptr, std::vector<SpmvTile> *out);
