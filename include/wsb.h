@@ -251,6 +251,27 @@ int wsb_matrix_create(wsb_context *ctx, uint32_t n, const uint32_t *row_ptr, con
                       uint64_t block_starts_len, int32_t layout, wsb_matrix **out);
 int wsb_matrix_info_get(const wsb_matrix *m, wsb_matrix_info *out);
 void wsb_matrix_destroy(wsb_matrix *m);
+/* Tile autotuner (no counterpart in the reference, whose kernels have one  */
+/* fixed launch shape): times the solver's SpMV and update kernels on this  */
+/* matrix for a few tile sizes (a short PCG run on b = ones), keeps the     */
+/* fastest of each, and records the choice for matrices of the same shape   */
+/* class (layout, n within a factor of 2, nonzeros per row) created later   */
+/* in this process. Retuned tiles regroup the FP64 partial sums of the dot  */
+/* products: results agree with the untuned ones to FP64 rounding.          */
+typedef struct wsb_tune_result {
+    uint32_t spmv_rows;          /* rows per SpMV tile (6 x block rows for BSR6) */
+    uint32_t spmv_cap;           /* nonzeros (CSR) or 6x6 blocks (BSR6) per SpMV tile */
+    uint32_t update_rows;        /* rows per update tile */
+    uint32_t update_blocks;      /* block starts per update tile */
+    double spmv_ms, update_ms;   /* mean kernel time with the chosen tiles */
+    double default_spmv_ms, default_update_ms;  /* ... with the largest tiles */
+    uint32_t candidates;         /* tilings timed */
+    uint32_t reserved;
+} wsb_tune_result;
+int wsb_matrix_autotune(wsb_context *ctx, wsb_matrix *m, uint32_t iterations, wsb_tune_result *out);
+/* Forgets the tilings the autotuner recorded per shape class. */
+void wsb_autotune_clear(void);
+
 /* Copies the block-Jacobi factors the handle holds (built on the device,   */
 /* num_blocks * 36 floats, the layout and bits of the Vec<f32> that         */
 /* build_lu_blocks_from_csr_block_starts_6 returns, compute.rs:84-181)      */

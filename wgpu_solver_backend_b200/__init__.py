@@ -374,6 +374,15 @@ class Matrix:
                                                C.byref(h)), ctx.handle)
         return Matrix(ctx, h)
 
+    def autotune(self, iterations: int = 8) -> dict:
+        """Times candidate tile sizes of the SpMV and update kernels on this
+        matrix, keeps the fastest and records them for matrices of the same
+        shape class created later (wsb_matrix_autotune)."""
+        r = _lib.TuneResult()
+        _check(_lib_handle().wsb_matrix_autotune(self.ctx.handle, self.handle, int(iterations), C.byref(r)),
+               self.ctx.handle)
+        return {k: getattr(r, k) for k, _ in _lib.TuneResult._fields_ if k != "reserved"}
+
     def lu(self) -> np.ndarray:
         """The block-Jacobi factors held on the device (num_blocks * 36
         floats, the layout of build_lu_blocks_from_csr_block_starts_6)."""
@@ -538,6 +547,11 @@ def lattice_sizes(side: int) -> dict:
     s = _lib.LatticeSizes()
     _check(_lib_handle().wsb_lattice_sizes_get(int(side), C.byref(s)))
     return {k: getattr(s, k) for k, _ in _lib.LatticeSizes._fields_}
+
+
+def autotune_clear() -> None:
+    """Forgets the tile sizes the autotuner recorded per shape class."""
+    _lib_handle().wsb_autotune_clear()
 
 
 def lattice_generate(side: int, seed: int = 0, aniso_log10: float = 0.0) -> dict:

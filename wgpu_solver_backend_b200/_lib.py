@@ -47,6 +47,13 @@ class MatrixInfo(C.Structure):
                 ("iteration_bytes", C.c_uint64)]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("spmv_rows", C.c_uint32), ("spmv_cap", C.c_uint32), ("update_rows", C.c_uint32),
+                ("update_blocks", C.c_uint32), ("spmv_ms", C.c_double), ("update_ms", C.c_double),
+                ("default_spmv_ms", C.c_double), ("default_update_ms", C.c_double), ("candidates", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("max_active", C.c_uint32), ("memory_budget_bytes", C.c_uint64),
                 ("iters_per_step", C.c_uint32), ("reserved", C.c_uint32)]
@@ -106,6 +113,8 @@ SIGNATURES = {
     "wsb_matrix_info_get": (C.c_int, [vp, C.POINTER(MatrixInfo)]),
     "wsb_matrix_destroy": (None, [vp]),
     "wsb_matrix_read_lu": (C.c_int, [vp, vp, f32p, C.c_uint64]),
+    "wsb_matrix_autotune": (C.c_int, [vp, vp, C.c_uint32, C.POINTER(TuneResult)]),
+    "wsb_autotune_clear": (None, []),
     "wsb_solve": (C.c_int, [vp, vp, f32p, f32p, C.c_uint64, C.c_float, C.c_float, C.POINTER(SolveOpts),
                             C.POINTER(SolveResult)]),
     "wsb_solve_device": (C.c_int, [vp, vp, vp, vp, C.c_uint64, C.c_float, C.c_float, C.POINTER(SolveOpts),

@@ -741,6 +741,15 @@ extern "C" int wsb_matrix_info_get(const wsb_matrix *m, wsb_matrix_info *out) {
     return WSB_OK;
 }
 
+extern "C" int wsb_matrix_autotune(wsb_context *ctx, wsb_matrix *m, uint32_t iterations, wsb_tune_result *out) {
+    CHECK_CTX(ctx);
+    if (!m) return fail(ctx, WSB_ERR_BAD_INPUT, "matrix is null");
+    m->eng.reset();  // its systems point at the tiles being replaced
+    return autotune_matrix(ctx, &m->A, &m->M, iterations, out);
+}
+
+extern "C" void wsb_autotune_clear(void) { tile_caps_clear(); }
+
 extern "C" int wsb_matrix_read_lu(wsb_context *ctx, const wsb_matrix *m, float *out, uint64_t out_len) {
     CHECK_CTX(ctx);
     if (!m || (!out && m->M.nb)) return fail(ctx, WSB_ERR_BAD_INPUT, "bad arguments");

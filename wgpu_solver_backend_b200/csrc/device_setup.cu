@@ -267,8 +267,12 @@ int prepare_system_device(Context *ctx, uint32_t n, const uint32_t *row_ptr, con
                     "BSR6 layout needs blocks of exactly 6 rows whose rows store complete 6x6 blocks with "
                     "strictly increasing columns");
     }
+    const TileCaps caps = tile_caps_for(bsr ? LAYOUT_BSR6 : LAYOUT_CSR, n, nnz);
+    M->h_bs.assign(bs, bs + bs_len);
+    M->tile_rows = caps.upd_rows;
+    M->tile_blocks = caps.upd_blocks;
     std::vector<UpdTile> utiles;
-    build_upd_tiles(n, bs, nb, &utiles);
+    build_upd_tiles(n, bs, nb, &utiles, caps.upd_rows, caps.upd_blocks);
     M->n_utiles = (uint32_t)utiles.size();
     if ((rc = dev_upload(ctx, &M->utiles, utiles.data(), utiles.size(), 1, st, &M->bytes))) {
         free_csr();
@@ -296,7 +300,8 @@ int prepare_system_device(Context *ctx, uint32_t n, const uint32_t *row_ptr, con
         A->bytes += sizeof(float) * (A->nbsr * 36 + kPadElems);
         k_prep_bsr6_fill<<<grid_of(6ull * nbr, 128, sms), 128, 0, st>>>(nbr, d_rp, d_col, d_val, A->bcol, A->bval);
         WSB_CUDA_TRY(ctx, cudaGetLastError());
-        build_spmv_tiles_bsr(nbr, brow_ptr.data(), &stiles);
+        build_spmv_tiles_bsr(nbr, brow_ptr.data(), &stiles, caps.spmv_rows / 6, caps.spmv_cap);
+        A->h_rows = std::move(brow_ptr);
         free_csr();
     } else {
         A->layout = LAYOUT_CSR;
@@ -322,8 +327,11 @@ int prepare_system_device(Context *ctx, uint32_t n, const uint32_t *row_ptr, con
         WSB_CUDA_TRY(ctx, cudaMemcpyAsync(A->col, d_col, nz_bytes, cudaMemcpyDeviceToDevice, st));
         WSB_CUDA_TRY(ctx, cudaMemcpyAsync(A->val, d_val, nz_bytes, cudaMemcpyDeviceToDevice, st));
         free_csr();
-        build_spmv_tiles_csr(n, row_ptr, &stiles);
+        build_spmv_tiles_csr(n, row_ptr, &stiles, caps.spmv_rows, caps.spmv_cap);
+        A->h_rows.assign(row_ptr, row_ptr + (size_t)n + 1);
     }
+    A->tile_rows = caps.spmv_rows;
+    A->tile_cap = caps.spmv_cap;
     A->n_stiles = (uint32_t)stiles.size();
     if ((rc = dev_upload(ctx, &A->stiles, stiles.data(), stiles.size(), 1, st, &A->bytes))) return rc;
     WSB_CUDA_TRY(ctx, cudaStreamSynchronize(st));

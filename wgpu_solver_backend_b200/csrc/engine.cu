@@ -79,8 +79,12 @@ int upload_matA(Context *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_
         if ((rc = upload(ctx, &out->brow_ptr, brow_ptr.data(), brow_ptr.size(), 8, st, &out->bytes))) return rc;
         if ((rc = upload(ctx, &out->bcol, bcol.data(), bcol.size(), kPadElems, st, &out->bytes))) return rc;
         if ((rc = upload(ctx, &out->bval, bval.data(), bval.size(), 16, st, &out->bytes))) return rc;
+        const TileCaps caps = tile_caps_for(LAYOUT_BSR6, n, nnz);
         std::vector<SpmvTile> tiles;
-        build_spmv_tiles_bsr(n / 6, brow_ptr.data(), &tiles);
+        build_spmv_tiles_bsr(n / 6, brow_ptr.data(), &tiles, caps.spmv_rows / 6, caps.spmv_cap);
+        out->h_rows = brow_ptr;
+        out->tile_rows = caps.spmv_rows;
+        out->tile_cap = caps.spmv_cap;
         out->n_stiles = (uint32_t)tiles.size();
         if ((rc = upload(ctx, &out->stiles, tiles.data(), tiles.size(), 1, st, &out->bytes))) return rc;
         WSB_CUDA_TRY(ctx, cudaStreamSynchronize(st));
@@ -90,8 +94,12 @@ int upload_matA(Context *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_
     if ((rc = upload(ctx, &out->row_ptr, row_ptr, (size_t)n + 1, 8, st, &out->bytes))) return rc;
     if ((rc = upload(ctx, &out->col, col, nnz, kPadElems, st, &out->bytes))) return rc;
     if ((rc = upload(ctx, &out->val, val, nnz, kPadElems, st, &out->bytes))) return rc;
+    const TileCaps caps = tile_caps_for(LAYOUT_CSR, n, nnz);
     std::vector<SpmvTile> tiles;
-    build_spmv_tiles_csr(n, row_ptr, &tiles);
+    build_spmv_tiles_csr(n, row_ptr, &tiles, caps.spmv_rows, caps.spmv_cap);
+    out->h_rows.assign(row_ptr, row_ptr + (size_t)n + 1);
+    out->tile_rows = caps.spmv_rows;
+    out->tile_cap = caps.spmv_cap;
     out->n_stiles = (uint32_t)tiles.size();
     if ((rc = upload(ctx, &out->stiles, tiles.data(), tiles.size(), 1, st, &out->bytes))) return rc;
     WSB_CUDA_TRY(ctx, cudaStreamSynchronize(st));
@@ -107,7 +115,10 @@ int upload_precond(Context *ctx, uint32_t n, const float *lu, const uint32_t *bs
     if ((rc = upload(ctx, &out->lu, lu, (size_t)out->nb * 36, 4, st, &out->bytes))) return rc;
     if ((rc = upload(ctx, &out->bs, bs, (size_t)bs_len, 8, st, &out->bytes))) return rc;
     std::vector<UpdTile> tiles;
-    build_upd_tiles(n, bs, out->nb, &tiles);
+    build_upd_tiles(n, bs, out->nb, &tiles, kUpdTileRows, kUpdBlocks);
+    out->h_bs.assign(bs, bs + bs_len);
+    out->tile_rows = kUpdTileRows;
+    out->tile_blocks = kUpdBlocks;
     out->n_utiles = (uint32_t)tiles.size();
     if ((rc = upload(ctx, &out->utiles, tiles.data(), tiles.size(), 1, st, &out->bytes))) return rc;
     WSB_CUDA_TRY(ctx, cudaStreamSynchronize(st));

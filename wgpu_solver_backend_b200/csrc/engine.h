@@ -22,6 +22,10 @@ struct MatA {
     SpmvTile *stiles = nullptr;
     uint32_t n_stiles = 0;
     uint64_t bytes = 0;
+    // Host copy of the row structure the SpMV tiles are cut from (row_ptr,
+    // or brow_ptr for BSR6) and the caps the current tiles were built with.
+    std::vector<uint32_t> h_rows;
+    uint32_t tile_rows = 0, tile_cap = 0;
     ~MatA();
 };
 
@@ -35,8 +39,28 @@ struct Precond {
     UpdTile *utiles = nullptr;
     uint32_t n_utiles = 0;
     uint64_t bytes = 0;
+    std::vector<uint32_t> h_bs;                 // host copy of the block starts
+    uint32_t tile_rows = 0, tile_blocks = 0;    // caps of the current update tiles
     ~Precond();
 };
+
+// SpMV and update tile caps (rows are rows for CSR and 6 x block rows for
+// BSR6; cap is nonzeros for CSR and 6x6 blocks for BSR6).
+struct TileCaps {
+    uint32_t spmv_rows, spmv_cap, upd_rows, upd_blocks;
+};
+// The caps recorded for matrices of this shape by the autotuner, or the
+// largest tiles the kernels stage.
+TileCaps tile_caps_for(uint32_t layout, uint32_t n, uint64_t nnz);
+void tile_caps_record(uint32_t layout, uint32_t n, uint64_t nnz, const TileCaps &c);
+void tile_caps_clear();
+// Rebuild a matrix's SpMV tiles or a preconditioner's update tiles with new
+// caps (device tile lists replaced; no solve may be running on them).
+int retile_spmv(MatA *A, uint32_t rows, uint32_t cap, cudaStream_t st);
+int retile_update(Precond *M, uint32_t rows, uint32_t blocks, cudaStream_t st);
+// Times candidate tilings of the matrix's SpMV and update kernels, keeps the
+// fastest of each and records them for the matrix's shape class (tune.cu).
+int autotune_matrix(Context *ctx, MatA *A, Precond *M, uint32_t iters, wsb_tune_result *out);
 
 // Host arrays of a system; csr is always given, the rest is derived.
 int upload_matA(Context *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_t *col, const float *val,

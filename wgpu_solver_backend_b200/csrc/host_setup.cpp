@@ -177,51 +177,62 @@ int validate_system(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, ui
     return WSB_OK;
 }
 
-// Greedy CSR row tiles: <= kSpmvTileRows rows and <= kCsrCap nonzeros (one TMA
-// stage), except a single row longer than kCsrCap, which gets a tile of its
-// own and is streamed through shared memory in chunks by the kernel.
-void build_spmv_tiles_csr(uint32_t n, const uint32_t *row_ptr, std::vector<SpmvTile> *out) {
+// Greedy CSR row tiles: <= max_rows rows and <= max_nnz nonzeros (bounded
+// by kSpmvTileRows and kCsrCap, one stage), except a single longer row,
+// which gets a tile of its own (beyond kCsrCap the kernel streams it in
+// chunks).
+void build_spmv_tiles_csr(uint32_t n, const uint32_t *row_ptr, std::vector<SpmvTile> *out, uint32_t max_rows,
+                          uint32_t max_nnz) {
     out->clear();
+    max_rows = std::max<uint32_t>(1, std::min<uint32_t>(max_rows, kSpmvTileRows));
+    max_nnz = std::max<uint32_t>(1, std::min<uint32_t>(max_nnz, kCsrCap));
     uint32_t r0 = 0;
     while (r0 < n) {
         uint32_t r1 = r0;
-        while (r1 < n && r1 - r0 < (uint32_t)kSpmvTileRows) {
+        while (r1 < n && r1 - r0 < max_rows) {
             const uint64_t tile_nnz = (uint64_t)row_ptr[r1 + 1] - row_ptr[r0];
-            if (r1 > r0 && tile_nnz > (uint64_t)kCsrCap) break;
+            if (r1 > r0 && tile_nnz > (uint64_t)max_nnz) break;
             ++r1;
-            if (tile_nnz > (uint64_t)kCsrCap) break;  // long single row
+            if (tile_nnz > (uint64_t)max_nnz) break;  // long single row
         }
         out->push_back({r0, r1, row_ptr[r0], row_ptr[r1]});
         r0 = r1;
     }
 }
 
-// BSR6 tiles over block rows: <= kSpmvTileRows/6 block rows and <= kBsrCapBlocks
-// blocks (a longer block row is chunked by the kernel).
-void build_spmv_tiles_bsr(uint32_t nbrows, const uint32_t *brow_ptr, std::vector<SpmvTile> *out) {
+// BSR6 tiles over block rows: <= max_brows block rows and <= max_blocks
+// blocks (bounded by kSpmvTileRows / 6 and kBsrCapBlocks; a block row longer
+// than kBsrCapBlocks is chunked by the kernel).
+void build_spmv_tiles_bsr(uint32_t nbrows, const uint32_t *brow_ptr, std::vector<SpmvTile> *out,
+                          uint32_t max_brows, uint32_t max_blocks) {
     out->clear();
-    const uint32_t max_brows = kSpmvTileRows / 6;
+    max_brows = std::max<uint32_t>(1, std::min<uint32_t>(max_brows, kSpmvTileRows / 6));
+    max_blocks = std::max<uint32_t>(1, std::min<uint32_t>(max_blocks, kBsrCapBlocks));
     uint32_t r0 = 0;
     while (r0 < nbrows) {
         uint32_t r1 = r0;
         while (r1 < nbrows && r1 - r0 < max_brows) {
             const uint64_t blocks = (uint64_t)brow_ptr[r1 + 1] - brow_ptr[r0];
-            if (r1 > r0 && blocks > (uint64_t)kBsrCapBlocks) break;
+            if (r1 > r0 && blocks > (uint64_t)max_blocks) break;
             ++r1;
-            if (blocks > (uint64_t)kBsrCapBlocks) break;
+            if (blocks > (uint64_t)max_blocks) break;
         }
         out->push_back({r0, r1, brow_ptr[r0], brow_ptr[r1]});
         r0 = r1;
     }
 }
 
-// Update tiles of <= kUpdTileRows rows holding <= kUpdBlocks block starts. A cut
-// is allowed at a block start or at a row whose position inside its block is
-// >= 6 (the reference never touches z there, block_jacobi.wgsl:79,124-126),
-// so the solved rows of a block are always inside one tile.
-void build_upd_tiles(uint32_t n, const uint32_t *bs, uint32_t nb, std::vector<UpdTile> *out) {
+// Update tiles of <= max_rows rows holding <= max_blocks block starts
+// (bounded by kUpdTileRows and kUpdBlocks). A cut is allowed at a block
+// start or at a row whose position inside its block is >= 6 (the reference
+// never touches z there, block_jacobi.wgsl:79,124-126), so the solved rows of
+// a block are always inside one tile.
+void build_upd_tiles(uint32_t n, const uint32_t *bs, uint32_t nb, std::vector<UpdTile> *out, uint32_t max_rows,
+                     uint32_t max_blocks) {
     out->clear();
     if (n == 0) return;
+    max_rows = std::max<uint32_t>(6, std::min<uint32_t>(max_rows, kUpdTileRows));
+    max_blocks = std::max<uint32_t>(1, std::min<uint32_t>(max_blocks, kUpdBlocks));
     std::vector<uint8_t> cut_ok(n + 1, 0);
     std::vector<uint32_t> starts_before(n + 1, 0);  // block starts in [0, r)
     cut_ok[n] = 1;
@@ -238,8 +249,8 @@ void build_upd_tiles(uint32_t n, const uint32_t *bs, uint32_t nb, std::vector<Up
     }
     uint32_t r0 = 0;
     while (r0 < n) {
-        uint32_t r1 = std::min<uint32_t>(n, r0 + kUpdTileRows);
-        while (r1 > r0 + 1 && (!cut_ok[r1] || starts_before[r1] - starts_before[r0] > (uint32_t)kUpdBlocks)) --r1;
+        uint32_t r1 = std::min<uint32_t>(n, r0 + max_rows);
+        while (r1 > r0 + 1 && (!cut_ok[r1] || starts_before[r1] - starts_before[r0] > max_blocks)) --r1;
         // r0 + 1 is always a cut when the block at r0 has one row or r0 is a
         // passive row; otherwise the loop stops at the next block start.
         while (!cut_ok[r1]) ++r1;

@@ -197,9 +197,13 @@ int build_lu_blocks_6(uint32_t n, const uint32_t *row_ptr, uint64_t row_ptr_len,
 int validate_system(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, uint64_t nnz,
                     const uint32_t *bs, uint64_t bs_len, std::string *err, bool check_cols = true);
 
-void build_spmv_tiles_csr(uint32_t n, const uint32_t *row_ptr, std::vector<SpmvTile> *out);
-void build_spmv_tiles_bsr(uint32_t nbrows, const uint32_t *brow_ptr, std::vector<SpmvTile> *out);
-void build_upd_tiles(uint32_t n, const uint32_t *bs, uint32_t nb, std::vector<UpdTile> *out);
+// Tile builders; the caps default to the largest tiles the kernels stage.
+void build_spmv_tiles_csr(uint32_t n, const uint32_t *row_ptr, std::vector<SpmvTile> *out,
+                          uint32_t max_rows = kSpmvTileRows, uint32_t max_nnz = kCsrCap);
+void build_spmv_tiles_bsr(uint32_t nbrows, const uint32_t *brow_ptr, std::vector<SpmvTile> *out,
+                          uint32_t max_brows = kSpmvTileRows / 6, uint32_t max_blocks = kBsrCapBlocks);
+void build_upd_tiles(uint32_t n, const uint32_t *bs, uint32_t nb, std::vector<UpdTile> *out,
+                     uint32_t max_rows = kUpdTileRows, uint32_t max_blocks = kUpdBlocks);
 // True when every block has 6 rows and every touched 6x6 block is fully stored.
 bool bsr6_convertible(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, const uint32_t *bs,
                       uint64_t bs_len);
