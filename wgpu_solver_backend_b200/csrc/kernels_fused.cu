@@ -878,8 +878,7 @@ __device__ __forceinline__ float staged_r(const float *stage, uint32_t o, float 
 // sflag.
 template <bool kInit>
 __device__ __forceinline__ void bj_stage(const UpdDesc &d, const float *stage, float *sz, uint32_t *sflag,
-                                         uint32_t tag) {
-    const uint32_t j = threadIdx.x;
+                                         uint32_t tag, uint32_t j) {
     if (j >= d.nblk) return;
     const uint32_t *bs = reinterpret_cast<const uint32_t *>(stage + kBsOff);
     const uint32_t off = bs[d.blk0 + j - d.ba], nxt = bs[d.blk0 + j + 1 - d.ba];
@@ -921,6 +920,73 @@ __device__ __forceinline__ void bj_stage(const UpdDesc &d, const float *stage, f
         }
 }
 
+// Barrier, reductions and ticket of one consumer group of the update
+// kernels: GT threads (local index lt) on named barrier BAR.
+template <int GT, int BAR>
+__device__ __forceinline__ void gsync() {
+    asm volatile("bar.sync %0, %1;" ::"n"(BAR), "n"(GT) : "memory");
+}
+
+template <int GT, int BAR>
+__device__ __forceinline__ double2 group_sum2(double a, double b, double *red, uint32_t lt) {
+    a = warp_sum(a);
+    b = warp_sum(b);
+    const uint32_t lane = lt & 31u, w = lt >> 5;
+    if (lane == 0) {
+        red[w] = a;
+        red[32 + w] = b;
+    }
+    gsync<GT, BAR>();
+    double sa = 0.0, sb = 0.0;
+    if (w == 0) {
+        sa = lane < (uint32_t)(GT >> 5) ? red[lane] : 0.0;
+        sb = lane < (uint32_t)(GT >> 5) ? red[32 + lane] : 0.0;
+        sa = warp_sum(sa);
+        sb = warp_sum(sb);
+    }
+    gsync<GT, BAR>();
+    return make_double2(sa, sb);
+}
+
+// Sum of n pairs of FP64 partials over the group: thread lt adds elements
+// lt, lt + GT, ... in that order (8 loads in flight), then the group sum.
+template <int GT, int BAR>
+__device__ __forceinline__ double2 group_sum_partials2(const double2 *__restrict__ p, uint32_t n, double *red,
+                                                       uint32_t lt) {
+    double va = 0.0, vb = 0.0;
+    uint32_t i = lt;
+    for (; i + 7u * GT < n; i += 8u * GT) {
+        double2 q[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) q[u] = __ldcg(p + i + u * GT);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            va += q[u].x;
+            vb += q[u].y;
+        }
+    }
+    for (; i < n; i += GT) {
+        const double2 q = __ldcg(p + i);
+        va += q.x;
+        vb += q.y;
+    }
+    return group_sum2<GT, BAR>(va, vb, red, lt);
+}
+
+template <int GT, int BAR>
+__device__ __forceinline__ bool group_ticket(uint32_t *counter, uint32_t cnt, uint32_t total, int *s_last,
+                                             uint32_t lt) {
+    if (lt == 0) {
+        __threadfence();
+        const uint32_t t = atomicAdd(counter, cnt);
+        *s_last = (t + cnt == total);
+    }
+    gsync<GT, BAR>();
+    const bool last = *s_last != 0;
+    if (last) __threadfence();
+    return last;
+}
+
 // The last CTA of a system's update tiles (kInit = false, k_update): r.r and
 // r.z from the per-tile partials in tile order, then the host-side logic of
 // compute.rs:466-488 on the device: breakdown checks (pAp == 0, then
@@ -928,15 +994,15 @@ __device__ __forceinline__ void bj_stage(const UpdDesc &d, const float *stage, f
 // beta = rz_new / rz_old, residual history entry. kInit = true (k_init):
 // b.b and rz_old; b.b == 0 finishes the system with 0 iterations and x
 // untouched (compute.rs:252-254), max_iter == 0 finishes it as not converged.
-template <bool kInit>
+template <bool kInit, int GT, int BAR>
 __device__ __forceinline__ void flush_upd(const SysDesc *__restrict__ sys, StepParams *sp, uint32_t s, uint32_t cnt,
-                                          double *red, int *s_last) {
+                                          double *red, int *s_last, uint32_t lt) {
     if (cnt == 0) return;
     const SysDesc &S = sys[s];
     SysState *st = S.st;
-    if (!take_ticket<NU>(&st->cnt_b, cnt, S.n_utiles, s_last)) return;
-    const double2 sum = sum_partials2<NU>(S.part_b, S.n_utiles, red);
-    if (threadIdx.x != 0) return;
+    if (!group_ticket<GT, BAR>(&st->cnt_b, cnt, S.n_utiles, s_last, lt)) return;
+    const double2 sum = group_sum_partials2<GT, BAR>(S.part_b, S.n_utiles, red, lt);
+    if (lt != 0) return;
     if (kInit) {
         st->bb = sum.x;
         st->rz_old = sum.y;
@@ -1008,8 +1074,9 @@ __device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, St
         if (base + lane * G < nw) it = work[base + lane * G];  // next batch, in flight
         __syncwarp();
         if (lane == 0) {
-            for (uint32_t i = 0; i <= cnt; ++i) {
-                if (i == cnt && more) break;
+            // After the last tile: one end marker for each consumer group.
+            const uint32_t n_out = more ? cnt : cnt + kUpdGroups;
+            for (uint32_t i = 0; i < n_out; ++i) {
                 const uint32_t s = k % NS;
                 if (k >= NS && !mbar_wait(&empty[s], ((k / NS) - 1) & 1u)) {
                     atomicOr(&sp->error, 32u);
@@ -1036,59 +1103,56 @@ __device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, St
     }
 }
 
+// Shared state of one consumer group of the update kernels.
+struct UpdGroupSmem {
+    float sz[kUpdTileRows];
+    uint32_t sflag[kUpdTileRows];
+    double red[64];
+    double2 wred[2 * (kUpdConsumers / kUpdGroups / 32)];
+    int s_last, s_ok[2];
+};
+
 // kInit = false (k_update): x += alpha p; r += (-alpha) Ap; z = M^-1 r; FP64
 // r.r and r.z per tile. kInit = true (k_init, after k_spmv_init):
 // r = b + (-1)(A x0); z = M^-1 r; p = z; FP64 b.b and r.z per tile
 // (compute.rs:226-331). Per-system results are formed by flush_upd.
-// Per tile the consumers pass two barriers: the stage wait (which also
-// separates the previous tile's warp partials from their publication by
-// thread 0) and the one between the block solves and the z writes.
-template <bool kInit>
-__device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, StepParams *sp, float *smem) {
+// The consumers form kUpdGroups independent groups of GT threads; group G
+// takes tiles G, G + kUpdGroups, ... of the ring (each thread kUpdTileRows /
+// GT rows of a tile), so one group's serial block solves overlap the other
+// group's row updates. Per tile a group passes two barriers of its own: the
+// stage wait (which also separates the previous tile's warp partials from
+// their publication by the group's thread 0) and the one between the block
+// solves and the z writes.
+template <bool kInit, int G>
+__device__ __forceinline__ void upd_consumers(const SysDesc *__restrict__ sys, StepParams *sp, float *smem,
+                                              uint64_t *full, uint64_t *empty, const UpdDesc *desc,
+                                              UpdGroupSmem &g) {
     constexpr uint32_t NS = kUpdStages;
-    __shared__ __align__(8) uint64_t full[NS], empty[NS];
-    __shared__ UpdDesc desc[NS];
-    __shared__ UpdDesc bdesc[32];
-    __shared__ float sz[kUpdTileRows];
-    __shared__ uint32_t sflag[kUpdTileRows];
-    __shared__ double red[64];
-    __shared__ double2 wred[2 * (NU / 32)];
-    __shared__ int s_last, s_ok[2];
-    const uint32_t tid = threadIdx.x;
-    if (tid == 0) {
-        for (uint32_t i = 0; i < NS; ++i) {
-            mbar_init(&full[i], 1);
-            mbar_init(&empty[i], NU / 32);
-        }
-        fence_barrier_init();
-    }
-    if (tid < kUpdTileRows) sflag[tid] = 0u;
-    __syncthreads();
-    pdl_start();
-    if (tid >= NU) {
-        if (tid < NU + 32) upd_producer<kInit>(sys, sp, smem, full, empty, desc, bdesc);
-        return;
-    }
+    constexpr int GT = NU / kUpdGroups;  // threads of the group
+    constexpr int BAR = 1 + G;           // its named barrier
+    constexpr uint32_t RPT = kUpdTileRows / GT;  // rows per thread
+    const uint32_t lt = threadIdx.x - G * GT;
     uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles of run_sys published since the last ticket
     double2 *pend_part = nullptr;                 // thread 0: partial slot of the tile in wred
     bool pend = false;
-    for (uint32_t k = 0;; ++k) {
+    uint32_t n = 0;  // tiles this group has taken
+    for (uint32_t k = G;; k += kUpdGroups, ++n) {
         const uint32_t s = k % NS, par = (k / NS) & 1u;
-        if (tid == 0) s_ok[k & 1u] = mbar_wait(&full[s], par) ? 1 : 0;
-        csync<NU>();
-        if (!s_ok[k & 1u]) {
-            if (tid == 0) atomicOr(&sp->error, kInit ? 4u : 2u);
+        if (lt == 0) g.s_ok[n & 1u] = mbar_wait(&full[s], par) ? 1 : 0;
+        gsync<GT, BAR>();
+        if (!g.s_ok[n & 1u]) {
+            if (lt == 0) atomicOr(&sp->error, kInit ? 4u : 2u);
             return;
         }
         mbar_observe(&full[s], par);
         // The descriptor is read in place: it stays valid until this stage
         // is handed back; what is needed after that is copied first.
         const UpdDesc &d = desc[s];
-        if (tid == 0 && pend) {
-            const double2 *wr = wred + (NU / 32) * ((k - 1) & 1u);
+        if (lt == 0 && pend) {
+            const double2 *wr = g.wred + (GT / 32) * ((n - 1) & 1u);
             double va = 0.0, vb = 0.0;
 #pragma unroll
-            for (int q = 0; q < NU / 32; ++q) {
+            for (int q = 0; q < GT / 32; ++q) {
                 va += wr[q].x;
                 vb += wr[q].y;
             }
@@ -1097,30 +1161,34 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
         }
         if (!d.valid) break;
         if (d.sys != run_sys) {
-            flush_upd<kInit>(sys, sp, run_sys, run_cnt, red, &s_last);
+            flush_upd<kInit, GT, BAR>(sys, sp, run_sys, run_cnt, g.red, &g.s_last, lt);
             run_sys = d.sys;
             run_cnt = 0;
         }
         float *stage = smem + s * kUpdStageFloats;
-        const uint32_t o = d.row0 - d.ra + tid;
         const float ma = -d.alpha;
-        float ri = 0.0f;
+        float ri[RPT];
         double da = 0.0;  // loop: r.r; init: b.b
-        if (tid < d.rows) {
-            const uint32_t i = d.row0 + tid;
-            ri = staged_r<kInit>(stage, o, ma);
-            if (kInit) {
-                const float bi = stage[o];
-                da = (double)bi * (double)bi;
-            } else {
-                const float xi = __fadd_rn(stage[o], __fmul_rn(d.alpha, stage[kVecCap + o]));
-                d.x[i] = xi;
-                da = (double)ri * (double)ri;
+#pragma unroll
+        for (uint32_t q = 0; q < RPT; ++q) {
+            const uint32_t t = lt + q * GT;
+            ri[q] = 0.0f;
+            if (t < d.rows) {
+                const uint32_t i = d.row0 + t, o = d.row0 - d.ra + t;
+                ri[q] = staged_r<kInit>(stage, o, ma);
+                if (kInit) {
+                    const float bi = stage[o];
+                    da += (double)bi * (double)bi;
+                } else {
+                    const float xi = __fadd_rn(stage[o], __fmul_rn(d.alpha, stage[kVecCap + o]));
+                    d.x[i] = xi;
+                    da += (double)ri[q] * (double)ri[q];
+                }
+                d.r[i] = ri[q];
             }
-            d.r[i] = ri;
         }
-        const uint32_t tag = k + 1;
-        bj_stage<kInit>(d, stage, sz, sflag, tag);
+        const uint32_t tag = n + 1;
+        bj_stage<kInit>(d, stage, g.sz, g.sflag, tag, lt);
         const uint32_t rows = d.rows, row0 = d.row0;
         float *const zv = d.z;
         float *const pv = d.p;
@@ -1128,28 +1196,62 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
         // Every thread is done reading the stage (it wrote nothing into it):
         // hand it back to the producer.
         mbar_arrive_warp(&empty[s]);
-        csync<NU>();
+        gsync<GT, BAR>();
         double rz = 0.0;
-        if (tid < rows) {
-            const uint32_t i = row0 + tid;
-            float zi;
-            if (sflag[tid] == tag) {
-                zi = sz[tid];
-                zv[i] = zi;
-            } else {
-                zi = zv[i];  // a row the block solve leaves alone (position >= 6 in its block)
+#pragma unroll
+        for (uint32_t q = 0; q < RPT; ++q) {
+            const uint32_t t = lt + q * GT;
+            if (t < rows) {
+                const uint32_t i = row0 + t;
+                float zi;
+                if (g.sflag[t] == tag) {
+                    zi = g.sz[t];
+                    zv[i] = zi;
+                } else {
+                    zi = zv[i];  // a row the block solve leaves alone (position >= 6 in its block)
+                }
+                if (kInit) pv[i] = zi;
+                rz += (double)ri[q] * (double)zi;
             }
-            if (kInit) pv[i] = zi;
-            rz = (double)ri * (double)zi;
         }
         da = warp_sum(da);
         rz = warp_sum(rz);
-        if ((tid & 31u) == 0) wred[(NU / 32) * (k & 1u) + (tid >> 5)] = make_double2(da, rz);
+        if ((lt & 31u) == 0) g.wred[(GT / 32) * (n & 1u) + (lt >> 5)] = make_double2(da, rz);
         pend = true;
         pend_part = part_slot;
         ++run_cnt;
     }
-    if (run_sys != 0xffffffffu) flush_upd<kInit>(sys, sp, run_sys, run_cnt, red, &s_last);
+    if (run_sys != 0xffffffffu) flush_upd<kInit, GT, BAR>(sys, sp, run_sys, run_cnt, g.red, &g.s_last, lt);
+}
+
+template <bool kInit>
+__device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, StepParams *sp, float *smem) {
+    constexpr uint32_t NS = kUpdStages;
+    __shared__ __align__(8) uint64_t full[NS], empty[NS];
+    __shared__ UpdDesc desc[NS];
+    __shared__ UpdDesc bdesc[32];
+    __shared__ UpdGroupSmem gsm[kUpdGroups];
+    const uint32_t tid = threadIdx.x;
+    if (tid == 0) {
+        for (uint32_t i = 0; i < NS; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], NU / kUpdGroups / 32);  // the warps of the one group that takes the stage
+        }
+        fence_barrier_init();
+    }
+    for (uint32_t i = tid; i < (uint32_t)kUpdGroups * kUpdTileRows; i += blockDim.x)
+        gsm[i / kUpdTileRows].sflag[i % kUpdTileRows] = 0u;
+    __syncthreads();
+    pdl_start();
+    if (tid >= NU) {
+        if (tid < NU + 32) upd_producer<kInit>(sys, sp, smem, full, empty, desc, bdesc);
+        return;
+    }
+    const uint32_t grp = tid / (NU / kUpdGroups);
+    if (grp == 0) upd_consumers<kInit, 0>(sys, sp, smem, full, empty, desc, gsm[0]);
+    if constexpr (kUpdGroups > 1) {
+        if (grp == 1) upd_consumers<kInit, 1>(sys, sp, smem, full, empty, desc, gsm[1]);
+    }
 }
 
 }  // namespace

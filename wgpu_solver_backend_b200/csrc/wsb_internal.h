@@ -43,9 +43,14 @@ namespace wsb {
 #ifndef WSB_UPD_BLOCKS
 #define WSB_UPD_BLOCKS 64
 #endif
+#ifndef WSB_UPD_GROUPS
+#define WSB_UPD_GROUPS 2
+#endif
 constexpr int kThreads = 256;        // threads per CTA of the vector and refinement kernels
 constexpr int kUpdConsumers = WSB_UPD_CONSUMERS;   // consumer threads per CTA of the update kernels
 constexpr int kUpdTileRows = kUpdConsumers;        // rows per update tile (<= kThreads)
+constexpr int kUpdGroups = WSB_UPD_GROUPS;         // independent consumer groups per update CTA (1 or 2)
+static_assert(kUpdGroups == 1 || kUpdGroups == 2, "update consumer groups");
 constexpr int kSpmvConsumers = WSB_SPMV_CONSUMERS;  // consumer threads per CTA of the SpMV kernels
 constexpr int kSpmvTileRows = kSpmvConsumers;       // rows (or block rows x 6) per SpMV tile
 constexpr int kCsrCap = WSB_CSR_CAP;         // CSR nonzeros per SpMV tile (one TMA stage)
