@@ -41,6 +41,20 @@ def peaks():
         return 6650.0, "fallback"
 
 
+# DRAM bytes per algorithmic byte of the SpMV kernel, from one ncu capture of
+# k_spmv_loop on the 56^3 lattice (BSR6 tiles, 206 MB of matrix > L2):
+# dram__bytes_read.sum 184.363 MB + dram__bytes_write.sum 7.223 MB over
+# 188.285 MB of algorithmic bytes. The kernel streams every byte once, so the
+# traffic scales with the launch's algorithmic bytes.
+SPMV_DRAM_PER_ALGO_BYTE = (184.363008e6 + 7.222784e6) / 188285444.0
+
+
+def spmv_traffic(algo_bytes):
+    return {"traffic": algo_bytes * SPMV_DRAM_PER_ALGO_BYTE,
+            "traffic_note": "dram read+write bytes per launch, scaled from an ncu capture of the same kernel on "
+                            "the 56^3 lattice (ratio %.4f to the algorithmic bytes)" % SPMV_DRAM_PER_ALGO_BYTE}
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
@@ -232,7 +246,7 @@ def run_plain(args, world, rank, local):
                 "d2h_bytes_per_step": 4 * n},
         "roofline": {"bound": "hbm", "kernel": "spmv (BSR6 tiles)" if info["layout"] == wsb.LAYOUT_BSR6 else "spmv",
                      "achieved": spmv_gbs, "peak": peak, "unit": "GB/s", "frac": spmv_gbs / peak,
-                     "peak_kind": peak_kind, "traffic": None,
+                     "peak_kind": peak_kind, **spmv_traffic(info["spmv_bytes"]),
                      "algorithmic_bytes_per_launch": info["spmv_bytes"], "launch_us": spmv_s * 1e6},
         "iteration_gbs": iter_gbs, "iteration_frac": iter_gbs / peak, "kernels": kernels,
         "gpu_launches": args.steps * (2 + 1 + 3 * iters),
@@ -462,7 +476,8 @@ def run_serve(args, world, rank, local):
                     "iterations_min_median_max": [int(min(iters)), int(np.median(iters)), int(max(iters))]},
         "roofline": {"bound": "hbm", "kernel": "k_spmv_loop (SpMV + p.Ap), largest system of the set",
                      "achieved": spmv_gbs, "peak": peak, "unit": "GB/s", "frac": spmv_gbs / peak,
-                     "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": info["spmv_bytes"],
+                     "peak_kind": peak_kind, **spmv_traffic(info["spmv_bytes"]),
+                     "algorithmic_bytes_per_launch": info["spmv_bytes"],
                      "launch_us": kt["spmv_ms"] * 1e3,
                      "update_kernel_gbs": upd_bytes / kt["update_ms"] / 1e6},
         "server": {"steps": st["steps"], "device_bytes_peak": st["device_bytes_peak"]},

@@ -5,9 +5,9 @@
 // = SMs x resident CTAs, grid-stride over the list), so one captured CUDA
 // graph serves any number of systems. The matrix and vector slices of a tile
 // are brought into shared memory with TMA bulk copies (cp.async.bulk +
-// mbarrier transaction counts) into a two-stage ring: while a CTA computes
-// tile k, tile k+1 is already streaming in, which keeps ~100 KB per SM in
-// flight. The gathered vector is read through the read-only path and stays
+// mbarrier transaction counts) into a ring of kSpmvStages (SpMV) or
+// kUpdStages (update) stages: while a CTA computes tile k, the next tiles
+// are already streaming in. The gathered vector is read through the read-only path and stays
 // in the 126 MB L2. Per-system reductions are deterministic: every tile
 // writes one FP64 partial and the last CTA of a system (ticket counter) sums
 // them in a fixed order, so a system's arithmetic does not depend on what
@@ -151,10 +151,13 @@ __device__ __forceinline__ void mbar_arrive_warp(uint64_t *bar) {
     if ((threadIdx.x & 31u) == 0) mbar_arrive(bar);
 }
 
-// The pipelined kernels run kThreads consumer threads (warps 0-7) and one
-// producer warp (plus a gather warp in the SpMV); consumers synchronise among
-// themselves on named barrier 1 so the other warps never have to join. Kernels without a
-// producer warp launch exactly kThreads threads and use the same barrier.
+// The pipelined kernels run their consumer threads in the low warps
+// (kSpmvConsumers in the SpMV, kUpdGroups groups of kUpdConsumers /
+// kUpdGroups in the update kernels), then one producer warp (plus the gather
+// warps in the SpMV). Consumers synchronise among themselves on named
+// barriers (1, and 2 for the second update group) so the other warps never
+// have to join. Kernels without a producer warp launch exactly kThreads
+// threads and use barrier 1.
 
 template <int N = kThreads>
 __device__ __forceinline__ void csync() {
