@@ -114,14 +114,22 @@ def dist_setup():
 
 
 def reduce_max(val, world):
+    """Maximum of a per-rank value over all ranks (the slowest rank's time)."""
     if world == 1:
         return val
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([val], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([val], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_rate(world, units_per_rank, slowest_s):
+    """Whole-job rate of `world` independent replicas that each process
+    `units_per_rank` units: all units over the slowest rank's time."""
+    return world * units_per_rank / slowest_s
 
 
 def barrier(world):
@@ -234,7 +242,7 @@ def run_plain(args, world, rank, local):
     torch.cuda.synchronize()
     e2e_s = reduce_max(time.perf_counter() - t0, world)
     line = {
-        "metric": METRIC, "value": world * args.steps / dev_s, "unit": "solves/s", "n_gpus": world,
+        "metric": METRIC, "value": replica_rate(world, args.steps, dev_s), "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 reductions)",
         "data": "synthetic 80^3 6-DOF lattice, seeded",
@@ -242,7 +250,7 @@ def run_plain(args, world, rank, local):
                    "layout": "BSR6" if info["layout"] == wsb.LAYOUT_BSR6 else "CSR",
                    "iterations": iters, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (matrix %.0f MB)" % (info["device_bytes"] / 1e6)},
-        "e2e": {"value": world * args.steps / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": 8 * n,
+        "e2e": {"value": replica_rate(world, args.steps, e2e_s), "unit": "solves/s", "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 4 * n},
         "roofline": {"bound": "hbm", "kernel": "spmv (BSR6 tiles)" if info["layout"] == wsb.LAYOUT_BSR6 else "spmv",
                      "achieved": spmv_gbs, "peak": peak, "unit": "GB/s", "frac": spmv_gbs / peak,
@@ -449,9 +457,9 @@ def run_serve(args, world, rank, local):
     peak, peak_kind = peaks()
     spmv_gbs = info["spmv_bytes"] / (kt["spmv_ms"] / 1e3) / 1e9
     upd_bytes = 28 * pool[big]["n"] + 144 * info["num_blocks"]
-    e2e = world * args.steps * R / e2e_s
+    e2e = replica_rate(world, args.steps * R, e2e_s)
     line = {
-        "metric": METRIC, "value": world * args.steps * R / dev_s, "unit": "solves/s", "n_gpus": world,
+        "metric": METRIC, "value": replica_rate(world, args.steps * R, dev_s), "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 reductions + f64 refinement)",
         "data": "synthetic 6-DOF lattice systems, seeded",

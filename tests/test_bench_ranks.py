@@ -1,0 +1,71 @@
+"""Multi-process logic of bench.py on CPU (gloo, world size 2): the path has
+no exchange step, so ranks are independent replicas that only meet for the
+barrier and the max-over-ranks time, and the reference arm runs on rank 0
+alone."""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+from conftest import ROOT
+
+sys.path.insert(0, ROOT)
+import bench  # noqa: E402
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out_dir):
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    try:
+        w, r, _ = bench.dist_setup()
+        bench.barrier(w)
+        # Per-rank "timed region": rank r takes 1.5 + r seconds for 3 steps.
+        slowest = bench.reduce_max(1.5 + r, w)
+        value = bench.replica_rate(w, 3, slowest)
+        bench.barrier(w)
+        with open(os.path.join(out_dir, f"rank{r}.json"), "w") as f:
+            json.dump({"world": w, "rank": r, "slowest": slowest, "value": value}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_replicas_take_the_slowest_rank_time_over_gloo(tmp_path):
+    world = 2
+    mp.start_processes(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    got = [json.load(open(tmp_path / f"rank{r}.json")) for r in range(world)]
+    for r, g in enumerate(got):
+        assert g["world"] == world and g["rank"] == r
+        assert g["slowest"] == 2.5                 # max over ranks, on every rank
+        assert g["value"] == pytest.approx(2 * 3 / 2.5)  # all ranks' units / slowest time
+
+
+def test_replica_rate_is_weak_scaling():
+    # Fixed work per rank: N ranks at the same time give N times the rate.
+    assert bench.replica_rate(1, 64, 2.0) == 32.0
+    assert bench.replica_rate(8, 64, 2.0) == 8 * 32.0
+
+
+@pytest.mark.parametrize("workload", ["serve", "plain80"])
+def test_reference_arm_runs_on_rank_zero_only(workload):
+    # A non-zero rank of the reference arm exits 0 at once, without output or work.
+    env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="2", MASTER_ADDR="127.0.0.1")
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--workload", workload], env=env, capture_output=True, text=True, timeout=120)
+    assert p.returncode == 0, p.stderr
+    assert p.stdout.strip() == ""
