@@ -1,9 +1,9 @@
 // Fused PCG kernels for sm_100a (declarations shared with the engine).
 //
 // One PCG iteration of every active system is three launches:
-//   k_spmv     Ap = A p (CSR or BSR6 tiles streamed through shared memory with
-//              128-bit loads), FP64 p.Ap per tile, and in the last CTA of each
-//              system: pAp, alpha = rz_old / pAp.
+//   k_spmv     Ap = A p (CSR or BSR6 tiles streamed through shared memory by
+//              TMA bulk copies, x gathered by cp.async), FP64 p.Ap per tile,
+//              and in the last CTA of each system: pAp, alpha = rz_old / pAp.
 //   k_update   x += alpha p, r -= alpha Ap, z = (LU)^-1 r per 6x6 block in
 //              registers, FP64 r.r and r.z per tile; the last CTA of each system
 //              computes beta, the stop test, the residual history and status.

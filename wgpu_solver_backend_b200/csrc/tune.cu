@@ -19,6 +19,7 @@
 #include <cmath>
 #include <map>
 #include <mutex>
+#include <string>
 #include <tuple>
 
 #include "engine.h"
@@ -118,8 +119,13 @@ static int time_tiling(Context *ctx, MatA *A, Precond *M, const float *d_b, uint
     int rc = E.add(A, M, cfg, &slot);
     if (rc) return rc;
     float *d_x0 = nullptr;
-    WSB_CUDA_TRY(ctx, cudaMallocAsync((void **)&d_x0, sizeof(float) * std::max<uint32_t>(A->n, 1), ctx->stream));
-    WSB_CUDA_TRY(ctx, cudaMemsetAsync(d_x0, 0, sizeof(float) * std::max<uint32_t>(A->n, 1), ctx->stream));
+    const size_t xbytes = sizeof(float) * std::max<uint32_t>(A->n, 1);
+    WSB_CUDA_TRY(ctx, cudaMallocAsync((void **)&d_x0, xbytes, ctx->stream));
+    const cudaError_t me = cudaMemsetAsync(d_x0, 0, xbytes, ctx->stream);
+    if (me != cudaSuccess) {
+        cudaFreeAsync(d_x0, ctx->stream);
+        return fail(ctx, WSB_ERR_CUDA, "autotune: cudaMemsetAsync failed: %s", cudaGetErrorString(me));
+    }
     rc = E.set_rhs(slot, d_b, d_x0, true);
     double ms[5] = {0, 0, 0, 0, 0};
     if (!rc) rc = E.profile_kernels(slot, iters, ms);
@@ -156,28 +162,37 @@ int wsb::autotune_matrix(Context *ctx, MatA *A, Precond *M, uint32_t iters, wsb_
     for (uint32_t d : {1u, 2u, 4u})
         if (kUpdTileRows / d >= 32) uc.push_back({kUpdTileRows / d, std::max(8u, (uint32_t)kUpdBlocks / d)});
     const TileCaps start{A->tile_rows, A->tile_cap, M->tile_rows, M->tile_blocks};
+    // On any failure the matrix goes back to the tiling it came with (the
+    // error of the failed step stays the reported one).
+    auto give_up = [&](int err) {
+        std::string msg;
+        {
+            std::lock_guard<std::mutex> lk(ctx->mu);
+            msg = ctx->last_error;
+        }
+        const int r1 = retile_spmv(A, start.spmv_rows, start.spmv_cap, ctx->stream);
+        const int r2 = retile_update(M, start.upd_rows, start.upd_blocks, ctx->stream);
+        if (r1 || r2) fail(ctx, err, "%s", msg.c_str());
+        return err;
+    };
     wsb_tune_result r{};
     int rc;
     // Defaults first (also the baseline the result reports).
     const TileCaps def = default_caps(A->layout);
     if ((rc = retile_spmv(A, def.spmv_rows, def.spmv_cap, ctx->stream)) ||
         (rc = retile_update(M, def.upd_rows, def.upd_blocks, ctx->stream)))
-        return rc;
+        return give_up(rc);
     double best_s = 0, best_u = 0;
-    if ((rc = time_tiling(ctx, A, M, d_b, iters, &best_s, &best_u))) {
-        retile_spmv(A, start.spmv_rows, start.spmv_cap, ctx->stream);
-        retile_update(M, start.upd_rows, start.upd_blocks, ctx->stream);
-        return rc;
-    }
+    if ((rc = time_tiling(ctx, A, M, d_b, iters, &best_s, &best_u))) return give_up(rc);
     r.default_spmv_ms = best_s;
     r.default_update_ms = best_u;
     r.candidates = 1;
     TileCaps best = def;
     for (const auto &c : sc) {
         if (c.first == def.spmv_rows && c.second == def.spmv_cap) continue;
-        if ((rc = retile_spmv(A, c.first, c.second, ctx->stream))) return rc;
+        if ((rc = retile_spmv(A, c.first, c.second, ctx->stream))) return give_up(rc);
         double s = 0, u = 0;
-        if ((rc = time_tiling(ctx, A, M, d_b, iters, &s, &u))) return rc;
+        if ((rc = time_tiling(ctx, A, M, d_b, iters, &s, &u))) return give_up(rc);
         ++r.candidates;
         if (s < best_s) {
             best_s = s;
@@ -185,12 +200,12 @@ int wsb::autotune_matrix(Context *ctx, MatA *A, Precond *M, uint32_t iters, wsb_
             best.spmv_cap = c.second;
         }
     }
-    if ((rc = retile_spmv(A, best.spmv_rows, best.spmv_cap, ctx->stream))) return rc;
+    if ((rc = retile_spmv(A, best.spmv_rows, best.spmv_cap, ctx->stream))) return give_up(rc);
     for (const auto &c : uc) {
         if (c.first == def.upd_rows && c.second == def.upd_blocks) continue;
-        if ((rc = retile_update(M, c.first, c.second, ctx->stream))) return rc;
+        if ((rc = retile_update(M, c.first, c.second, ctx->stream))) return give_up(rc);
         double s = 0, u = 0;
-        if ((rc = time_tiling(ctx, A, M, d_b, iters, &s, &u))) return rc;
+        if ((rc = time_tiling(ctx, A, M, d_b, iters, &s, &u))) return give_up(rc);
         ++r.candidates;
         if (u < best_u) {
             best_u = u;
@@ -198,7 +213,7 @@ int wsb::autotune_matrix(Context *ctx, MatA *A, Precond *M, uint32_t iters, wsb_
             best.upd_blocks = c.second;
         }
     }
-    if ((rc = retile_update(M, best.upd_rows, best.upd_blocks, ctx->stream))) return rc;
+    if ((rc = retile_update(M, best.upd_rows, best.upd_blocks, ctx->stream))) return give_up(rc);
     tile_caps_record(A->layout, A->n, A->nnz, best);
     r.spmv_rows = best.spmv_rows;
     r.spmv_cap = best.spmv_cap;

@@ -189,7 +189,7 @@ int dev_alloc(Context *ctx, void **p, size_t bytes, bool zero, cudaStream_t stre
 void dev_free(void *p);
 
 // ---------------------------------------------------------------------------
-// Host-side setup helpers (lu.cpp, tiles.cpp)
+// Host-side setup helpers (host_setup.cpp)
 // ---------------------------------------------------------------------------
 int lu_factor_inplace_6(float *mat, uint32_t n, uint32_t *pivot_k);
 // Returns WSB_OK / WSB_ERR_BAD_INPUT / WSB_ERR_ZERO_PIVOT with message in *err.
