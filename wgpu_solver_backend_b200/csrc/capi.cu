@@ -851,8 +851,13 @@ extern "C" int wsb_matrix_kernel_times(wsb_context *ctx, wsb_matrix *m, const fl
     int rc = E.add(&m->A, &m->M, cfg, &slot);
     if (rc) return rc;
     float *d_x0 = nullptr;
-    WSB_CUDA_TRY(ctx, cudaMallocAsync((void **)&d_x0, sizeof(float) * std::max<uint32_t>(m->A.n, 1), ctx->stream));
-    WSB_CUDA_TRY(ctx, cudaMemsetAsync(d_x0, 0, sizeof(float) * std::max<uint32_t>(m->A.n, 1), ctx->stream));
+    const size_t xbytes = sizeof(float) * std::max<uint32_t>(m->A.n, 1);
+    WSB_CUDA_TRY(ctx, cudaMallocAsync((void **)&d_x0, xbytes, ctx->stream));
+    const cudaError_t me = cudaMemsetAsync(d_x0, 0, xbytes, ctx->stream);
+    if (me != cudaSuccess) {
+        cudaFreeAsync(d_x0, ctx->stream);
+        return fail(ctx, WSB_ERR_CUDA, "kernel times: cudaMemsetAsync failed: %s", cudaGetErrorString(me));
+    }
     rc = E.set_rhs(slot, d_b, d_x0, true);
     if (!rc) rc = E.profile_kernels(slot, iterations, ms);
     cudaFreeAsync(d_x0, ctx->stream);
