@@ -16,6 +16,7 @@ import subprocess
 import numpy as np
 import pytest
 
+import oracle
 from conftest import BIN, COMPARE_X_GATES, GOLDEN, load_case
 
 CLI = os.path.join(BIN, "wgpu_solver_backend_cli")
@@ -216,7 +217,7 @@ def test_info_prints_adapter_and_metrics():
 def test_run_pcg_case_then_compare_x(tmp_path, k, precision):
     """commands.txt:26-78 end to end: solve at rel 1e-4, abs 1e-7, max 2000,
     then compare-x against x_ref with the dataset's gate."""
-    _, _, fx = load_case(k)
+    case, _, fx = load_case(k)
     out_x, out_m = tmp_path / "out" / "x.bin", tmp_path / "out" / "metrics.json"
     r = run(CLI, "--backend", "auto", "run-pcg-case", "--case-dir", os.path.join(GOLDEN, f"case_{k}"),
             "--max-iters", "2000", "--rel-tol", "1e-4", "--abs-tol", "1e-7", "--out-x", out_x,
@@ -234,6 +235,15 @@ def test_run_pcg_case_then_compare_x(tmp_path, k, precision):
         np.testing.assert_array_equal(wio.load_vector_bin(str(out_x)), fx["x"])
     else:
         assert abs(m["iterations"] - it_oracle) <= max(2, 0.02 * it_oracle)
+    # This implementation's result checks in the `solver` object: the true
+    # FP64 residual of the written x and one iteration's algorithmic bytes.
+    from wgpu_solver_backend_b200 import io as wio
+
+    xs = wio.load_vector_bin(str(out_x))
+    tr = oracle.true_relres_f64(case.a.row_ptr, case.a.col_idx, case.a.values, case.b, xs)
+    assert m["solver"]["final_relres_true_f64"] == pytest.approx(tr, rel=1e-9)
+    n, nnz, nb = case.a.n_rows, case.a.nnz, len(case.block_starts) - 1
+    assert m["solver"]["iteration_bytes"] == 8 * nnz + 4 * (n + 1) + 48 * n + 144 * nb
     rel, atol = COMPARE_X_GATES[k]
     c = run(CLI, "compare-x", "--x-ref", os.path.join(GOLDEN, f"case_{k}", "x_ref.bin"), "--x", out_x,
             "--rel-tol", rel, "--abs-tol", atol, "--top-k", "10")
@@ -249,5 +259,6 @@ def test_run_pcg_case_failure_is_reported_in_metrics(tmp_path):
     assert r.returncode == 0
     m = json.loads(out_m.read_text())
     assert m["converged"] is False and m["iterations"] is None and "did not converge" in m["error"]
+    assert m["solver"]["final_relres_true_f64"] is None and m["solver"]["gbps"] is None
     assert not out_x.exists()
     assert r.stderr.startswith("Solve failed: ")

@@ -370,4 +370,21 @@ std::string now_utc_rfc3339() {
     return s + "Z";
 }
 
+double true_relres_f64(const CsrMatrixBin &a, const std::vector<float> &b, const std::vector<float> &x) {
+    double rr = 0.0, bb = 0.0;
+    for (uint32_t i = 0; i < a.n_rows; ++i) {
+        double ax = 0.0;
+        for (uint32_t k = a.row_ptr[i]; k < a.row_ptr[i + 1]; ++k)
+            ax += (double)a.values[k] * (double)x[a.col_idx[k]];
+        const double r = (double)b[i] - ax;
+        rr += r * r;
+        bb += (double)b[i] * (double)b[i];
+    }
+    return bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
+}
+
+uint64_t pcg_iteration_bytes_csr(uint64_t n, uint64_t nnz, uint64_t num_blocks) {
+    return 8 * nnz + 4 * (n + 1) + 8 * n + 28 * n + 12 * n + 144 * num_blocks;
+}
+
 }  // namespace wsbcli

@@ -67,4 +67,16 @@ std::string json_str(const std::string &s);
 // without trailing zeros, 'Z' suffix).
 std::string now_utc_rfc3339();
 
+// ---- solve metrics ---------------------------------------------------------
+// True relative residual ||b - A x|| / ||b|| in FP64 (matrix and vectors
+// widened from f32, rows summed in index order); 0 when b == 0. The caller
+// guarantees sizes that match the matrix (a loaded, validated case).
+double true_relres_f64(const CsrMatrixBin &a, const std::vector<float> &b, const std::vector<float> &x);
+// Algorithmic HBM bytes of one PCG iteration on a CSR matrix, as the
+// library's wsb_matrix_info counts them: the SpMV (8 nnz + 4 (n + 1) + 8 n:
+// values, columns, row pointers, x read, y written), the update (x, p, r, Ap
+// read, x, r, z written: 28 n), p = z + beta p (12 n) and the 6x6 LU factors
+// (144 bytes per block; 24 n for blocks of 6 rows).
+uint64_t pcg_iteration_bytes_csr(uint64_t n, uint64_t nnz, uint64_t num_blocks);
+
 }  // namespace wsbcli

@@ -64,6 +64,7 @@ void print_help() {
         "run-pcg-case: --case-dir DIR --out-x PATH --out-metrics PATH [--max-iters 2000]\n"
         "              [--rel-tol 1e-8] [--abs-tol 0] [--precision f32-f64dot|reference-f32|mixed]\n"
         "              [--target-relres 1e-10] [--layout executors|auto|csr|bsr6] [--out-history PATH]\n"
+        "              [--hbm-peak-gbs 7700]\n"
         "compare-x:    --x-ref PATH --x PATH [--rel-tol 1e-3] [--abs-tol 1e-4] [--top-k 10]\n");
 }
 
@@ -341,6 +342,8 @@ struct SolveOut {
     wsb_solve_result res{};
     std::vector<double> history;
     long long load_ms = 0, setup_ms = 0;
+    CaseInputBin input;           // the loaded case (kept for the residual check)
+    uint64_t iteration_bytes = 0; // algorithmic HBM bytes of one PCG iteration
 };
 
 // Loads the case, builds the executors and LU (as run_pcg_case does) and
@@ -348,7 +351,7 @@ struct SolveOut {
 std::string run_pcg_case(wsb_context *ctx, const Args &a, uint64_t max_iters, float rel, float abs_tol,
                          SolveOut *o) {
     const auto t_load = Clock::now();
-    CaseInputBin c;
+    CaseInputBin &c = o->input;
     std::string e = load_case_dir(get(a, "case-dir", ""), &c);
     o->load_ms = ms_since(t_load);
     if (!e.empty()) return e;
@@ -388,6 +391,7 @@ std::string run_pcg_case(wsb_context *ctx, const Args &a, uint64_t max_iters, fl
             return wsb_last_error(ctx);
         }
         o->setup_ms = ms_since(t_setup);
+        o->iteration_bytes = pcg_iteration_bytes_csr(n, c.a.nnz, c.block_starts.size() - 1);
         rc = wsb_pcg_block_jacobi_csr(ctx, n, c.b.data(), n, o->x.data(), n, max_iters, rel, abs_tol, spmv, bj, &opts,
                                       &o->iterations, &o->res);
         e = rc ? wsb_last_error(ctx) : "";
@@ -403,6 +407,8 @@ std::string run_pcg_case(wsb_context *ctx, const Args &a, uint64_t max_iters, fl
                                     c.block_starts.data(), c.block_starts.size(), lay, &m)))
             return wsb_last_error(ctx);
         o->setup_ms = ms_since(t_setup);
+        wsb_matrix_info info;
+        if (wsb_matrix_info_get(m, &info) == WSB_OK) o->iteration_bytes = info.iteration_bytes;
         rc = wsb_solve(ctx, m, c.b.data(), o->x.data(), max_iters, rel, abs_tol, &opts, &o->res);
         e = rc ? wsb_last_error(ctx) : "";
         o->iterations = o->res.iterations;
@@ -456,6 +462,14 @@ int cmd_run_pcg_case(const Args &a) {
         }
     }
     const long long write_ms = ms_since(t_write0);
+    // Host-side checks of the result, outside the timed phases: the true FP64
+    // relative residual of x, and the PCG iterations' achieved HBM bandwidth
+    // (algorithmic bytes x iterations / device time) against --hbm-peak-gbs.
+    const double true_relres = converged ? true_relres_f64(o.input.a, o.input.b, o.x) : NAN;
+    const double peak_gbs = atof(get(a, "hbm-peak-gbs", "7700").c_str());
+    const double gbps = converged && o.res.device_ms > 0.0
+                            ? (double)o.iteration_bytes * (double)o.iterations / (o.res.device_ms * 1e6)
+                            : NAN;
     wsb_adapter_info ai;
     wsb_context_adapter_info(ctx, &ai);
     Json j;
@@ -489,6 +503,11 @@ int cmd_run_pcg_case(const Args &a) {
     j.raw("final_r_norm2", json_f64(o.res.final_r_norm2));
     j.raw("final_relres", json_f64(o.res.final_relres));
     j.raw("refine_sweeps", std::to_string(o.res.refine_sweeps));
+    j.raw("final_relres_true_f64", json_f64(true_relres));
+    j.raw("iteration_bytes", std::to_string(o.iteration_bytes));
+    j.raw("gbps", json_f64(gbps));
+    j.raw("roofline_peak_gbs", json_f64(peak_gbs));
+    j.raw("roofline_fraction", json_f64(peak_gbs > 0.0 ? gbps / peak_gbs : NAN));
     j.close();
     j.close();
     const std::string we = write_text_file(out_metrics, j.s);
