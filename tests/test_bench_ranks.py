@@ -1,7 +1,7 @@
 """Multi-process logic of bench.py on CPU (gloo, world size 2): the path has
 no exchange step, so ranks are independent replicas that only meet for the
 barrier and the max-over-ranks time, and the reference arm runs on rank 0
-alone."""
+alone. Also the reference arm's JSON line, which needs no GPU."""
 import json
 import os
 import socket
@@ -69,3 +69,20 @@ def test_reference_arm_runs_on_rank_zero_only(workload):
                         "--workload", workload], env=env, capture_output=True, text=True, timeout=120)
     assert p.returncode == 0, p.stderr
     assert p.stdout.strip() == ""
+
+
+def test_reference_arm_line_on_one_rank():
+    # The reference arm runs on host cores only: its JSON line carries the
+    # contract's keys, the CPU baseline it measured and a zero-copy e2e.
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE")}
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "0"], env=env, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    lines = [ln for ln in p.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == bench.METRIC and d["unit"] == "solves/s"
+    assert d["higher_is_better"] is True and d["n_gpus"] == 1 and d["steps"] == 1
+    assert d["value"] > 0 and d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["kind"] == "port"
+    assert d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"] == {"value": d["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
