@@ -113,3 +113,47 @@ def test_case_dir_round_trip_and_validation():
             f.write(b"\0")
         with pytest.raises(ValueError, match="trailing bytes"):
             wio.load_case_dir(d)
+
+
+def _random_csr(rng, n, density):
+    """Random square CSR with unsorted columns, duplicate entries in a row
+    (the LU extraction keeps the later one) and some exact zeros."""
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        k = int(rng.binomial(n, density))
+        cs = list(rng.integers(0, n, k)) + [i]
+        if rng.random() < 0.3 and cs:
+            cs.append(cs[0])  # a duplicate
+        rng.shuffle(cs)
+        for c in cs:
+            rows.append(i)
+            cols.append(int(c))
+            v = float(rng.normal()) if rng.random() > 0.05 else 0.0
+            vals.append(v + (4.0 if c == i and rng.random() > 0.1 else 0.0))
+    rp = np.zeros(n + 1, np.uint32)
+    np.add.at(rp, np.array(rows) + 1, 1)
+    return np.cumsum(rp).astype(np.uint32), np.array(cols, np.uint32), np.array(vals, np.float32)
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_host_lu_builder_matches_oracle_on_random_systems(seed):
+    """build_lu_blocks_from_csr_block_starts_6 (compute.rs:84-181) against
+    the oracle's restatement on random systems: blocks of 1..9 rows, unsorted
+    and duplicate columns, exact zeros. Same status, same first zero pivot
+    (block order), and the same factor bits when it succeeds."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(1, 60))
+    rp, ci, v = _random_csr(rng, n, float(rng.uniform(0.02, 0.3)))
+    cuts = [0]
+    while cuts[-1] < n:
+        cuts.append(min(n, cuts[-1] + int(rng.integers(1, 10))))
+    bs = np.array(cuts, np.uint32)
+    st, lu_o, bad, pk = oracle.build_lu_blocks_6(n, rp, ci, v, bs)
+    if st == oracle.OK:
+        lu = wsb.build_lu_blocks_from_csr_block_starts_6(n, rp, ci, v, bs)
+        assert np.array_equal(lu.view(np.uint32), lu_o.view(np.uint32))
+    else:
+        assert st == oracle.ZERO_PIVOT
+        with pytest.raises(wsb.WsbError) as e:
+            wsb.build_lu_blocks_from_csr_block_starts_6(n, rp, ci, v, bs)
+        assert e.value.status == _lib.ZERO_PIVOT and f"LU zero pivot at k = {pk}" in str(e.value)
