@@ -95,6 +95,44 @@ def test_text_to_bin_refuses_an_existing_dir_without_force(tmp_path):
     assert r.returncode == 0 and not (out / "stale.txt").exists()
 
 
+@pytest.mark.parametrize("seed", range(6))
+def test_text_to_bin_round_trip_of_random_systems(tmp_path, seed):
+    """Random lattice systems written with varying tokens per line (the
+    parser reads whitespace-separated tokens, convert_cli main.rs:104-401):
+    the binaries load back to the same arrays, bit for bit."""
+    from types import SimpleNamespace
+
+    from wgpu_solver_backend_b200 import io as wio
+    import wgpu_solver_backend_b200 as wsb
+
+    rng = np.random.default_rng(seed)
+    s = wsb.lattice_generate(int(rng.integers(1, 5)), seed=seed)
+    n = s["n"]
+    a = SimpleNamespace(n_rows=n, nnz=len(s["values"]), row_ptr=s["row_ptr"], col_idx=s["col_idx"],
+                        values=s["values"])
+    x0 = rng.normal(size=n).astype(np.float32)
+    x_ref = rng.normal(size=n).astype(np.float32)
+    case = SimpleNamespace(a=a, b=s["b"], x0=x0, block_starts=s["block_starts"])
+    txt = tmp_path / "ds.txt"
+    per_line = int(rng.integers(1, 40))
+    parts = ["# dataset (text)", f"n {n}", f"nnz {a.nnz}", ""]
+    for name, arr in [("row_ptr_u32", a.row_ptr), ("col_idx_u32", a.col_idx), ("values_f32", a.values),
+                      ("b_f32", case.b), ("x0_f32", x0), ("block_starts_u32", case.block_starts),
+                      ("x_ref_f32", x_ref)]:
+        parts += [name, f"len {len(arr)}", _tokens(np.asarray(arr), per_line), ""]
+    txt.write_text("\n".join(parts))
+    out = tmp_path / "case"
+    r = run(CONVERT, "text-to-bin", "--input", txt, "--out-dir", out)
+    assert r.returncode == 0, r.stderr
+    c = wio.load_case_dir(str(out))
+    for got, want in [(c.a.row_ptr, a.row_ptr), (c.a.col_idx, a.col_idx), (c.a.values, a.values), (c.b, case.b),
+                      (c.x0, x0), (c.block_starts, case.block_starts), (wio.load_vector_bin(str(out / "x_ref.bin")),
+                                                                          x_ref)]:
+        assert np.array_equal(np.asarray(got).view(np.uint32), np.asarray(want).view(np.uint32))
+    meta = json.loads((out / "meta.json").read_text())
+    assert meta["n"] == n and meta["nnz"] == a.nnz and meta["x_ref_present"] is True
+
+
 @pytest.mark.parametrize("text,msg", [
     ("nnz 1\nrow_ptr_u32\nlen 2\n0 1\n", "Missing 'n'"),
     ("n 1\nnnz 1\nrow_ptr_u32\nlen 3\n0 1\n", "Section row_ptr_u32: EOF while reading values (got 2, need 3)"),
