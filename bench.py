@@ -318,39 +318,91 @@ def served_pass(srv, pool, arrivals=None):
     return mk, [r[1]["total_ms"] for r in res], [r[1] for r in res]
 
 
-def cpu_baseline_serve(pool, sample_iters=200):
-    """The oracle's FP32 restatement of the reference solve (all host threads)
-    timed for a few PCG iterations on every request of the set, scaled by the
-    reference algorithm's own iteration count for that request at relative
-    tolerance 1e-8 (oracle/serve_reference_iterations.json)."""
+def serve_set(max_side=None):
+    """The requests of the serving set whose lattice side is at most max_side
+    (all of them by default)."""
+    max_side = SERVE["side_max"] if max_side is None else max_side
+    return [(sd, seed) for sd, seed in serve_requests() if sd <= max_side]
+
+
+def reference_pool(max_side=None):
+    """The serving request set generated by the oracle's own statement of the
+    lattice generator (bit-identical to the product's), so that the reference
+    process never loads the product library."""
     import oracle
 
-    import wgpu_solver_backend_b200 as wsb
+    pool = []
+    for side, seed in serve_set(max_side):
+        s = oracle.lattice_generate(side, seed, SERVE["aniso"])
+        s["side"], s["seed"] = side, seed
+        pool.append(s)
+    return pool
 
-    path = os.path.join(ROOT, "oracle", "serve_reference_iterations.json")
-    if not os.path.exists(path):
-        return {"value": None, "unit": "solves/s", "cores": oracle.num_threads(), "kind": "port",
-                "sample": "unavailable: oracle/serve_reference_iterations.json missing"}
-    with open(path) as f:
-        ref = {(r["side"], r["seed"]): r for r in json.load(f)["requests"]}
-    total_s, measured_s, iters_total = 0.0, 0.0, 0
-    for s in pool:
-        key = (s["side"], s["seed"])
-        n = s["n"]
-        lu = wsb.build_lu_blocks_from_csr_block_starts_6(n, s["row_ptr"], s["col_idx"], s["values"],
-                                                         s["block_starts"])
-        t0 = time.perf_counter()
-        r = oracle.pcg_ref_f32(s["row_ptr"], s["col_idx"], s["values"], lu, s["block_starts"], s["b"],
-                               np.zeros(n, np.float32), sample_iters, SERVE["target"], 0.0)
-        dt = time.perf_counter() - t0
-        measured_s += dt
-        it = ref[key]["iterations"]
-        iters_total += it
-        total_s += dt / max(1, r["iterations"]) * it
-    return {"value": len(pool) / total_s, "unit": "solves/s", "cores": oracle.num_threads(), "kind": "port",
-            "sample": f"{sample_iters} oracle FP32 PCG iterations on each of the {len(pool)} requests "
-                      f"({measured_s:.1f} s, {oracle.num_threads()} threads), scaled by the reference "
-                      f"algorithm's iteration count per request at rel 1e-8 ({iters_total} in all)"}
+
+REFERENCE_STOP = ("FP32 recursive residual r.r <= (1e-8)^2 b.b, the reference's stop test "
+                  "(compute.rs:481), max 60000 iterations")
+
+
+def reference_solve_requests(pool, idx):
+    """Complete CPU solves of pool[i], i in idx, by the reference algorithm:
+    the host LU build (compute.rs:37-181) and the FP32 PCG with the 256-wide
+    tree reductions (compute.rs:189-495), both restated in the oracle; all host
+    threads. Returns (seconds, lu_seconds, results)."""
+    import oracle
+
+    t0 = time.perf_counter()
+    systems = []
+    for i in idx:
+        s = pool[i]
+        st, lu, _, _ = oracle.build_lu_blocks_6(s["n"], s["row_ptr"], s["col_idx"], s["values"], s["block_starts"])
+        if st != oracle.OK:
+            raise RuntimeError(f"oracle LU failed on request {i} (status {st})")
+        systems.append(dict(s, lu=lu))
+    t1 = time.perf_counter()
+    res = oracle.pcg_ref_f32_many(systems, SERVE["max_iter"], SERVE["target"], 0.0)
+    return time.perf_counter() - t0, t1 - t0, res
+
+
+def repo_libraries():
+    """Shared objects of this repository mapped into the current process."""
+    found = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for ln in f:
+                path = ln.split()[-1] if ln.strip() else ""
+                if path.startswith(ROOT) and ".so" in os.path.basename(path):
+                    found.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(found)
+
+
+def side_note(args):
+    return "" if args.max_side >= SERVE["side_max"] else f", only sides <= {args.max_side}"
+
+
+def step_groups(n_req, steps):
+    """Requests solved by each of `steps` timed steps: contiguous groups that
+    together cover the set once (or one request per step, cycling, when there
+    are more steps than requests)."""
+    if steps <= n_req:
+        return [list(map(int, g)) for g in np.array_split(np.arange(n_req), steps)]
+    return [[k % n_req] for k in range(steps)]
+
+
+def cpu_baseline_serve(pool, stride=4):
+    """The reference algorithm on the host cores (oracle, all threads):
+    complete LU + FP32 PCG solves of every `stride`-th request of the set."""
+    import oracle
+
+    idx = list(range(0, len(pool), stride))
+    dt, lu_s, res = reference_solve_requests(pool, idx)
+    conv = sum(1 for r in res if r["status"] == oracle.OK)
+    return {"value": len(idx) / dt, "unit": "solves/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"complete solves (LU + PCG) of every {stride}th request of the set ({len(idx)} requests, "
+                      f"{sum(pool[i]['n'] for i in idx)} of {sum(p['n'] for p in pool)} unknowns), "
+                      f"{dt:.1f} s ({lu_s:.2f} s LU), {oracle.num_threads()} threads; {conv} of {len(idx)} "
+                      f"converged; stop: {REFERENCE_STOP}"}
 
 
 def run_serve(args, world, rank, local):
@@ -363,7 +415,7 @@ def run_serve(args, world, rank, local):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
-    reqs = serve_requests()
+    reqs = serve_set(args.max_side)
     t_gen = time.perf_counter()
     pool = []
     for side, seed in reqs:
@@ -463,8 +515,8 @@ def run_serve(args, world, rank, local):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 reductions + f64 refinement)",
         "data": "synthetic 6-DOF lattice systems, seeded",
-        "config": {"workload": f"serve: {R} requests, lattice side log-uniform [4,64] (n 384..1,572,864, "
-                               f"{n_total} unknowns in all), anisotropy 10^U(-2,2), true FP64 relres 1e-8 "
+        "config": {"workload": f"serve: {R} requests, lattice side log-uniform [4,64]{side_note(args)} "
+                               f"(n 384..1,572,864, {n_total} unknowns in all), anisotropy 10^U(-2,2), true FP64 relres 1e-8 "
                                f"by FP64 refinement around FP32 PCG",
                    "step": "one pass over the request set", "value_path": "resident batch (wsb_batch)",
                    "e2e_path": "continuous-batching server (wsb_server, host arrays)",
@@ -501,26 +553,45 @@ def run_serve(args, world, rank, local):
 
 
 def run_reference_serve(args, world, rank, local):
-    reqs = serve_requests()
-    pool = []
-    for side, seed in reqs:
-        sysm = serve_system(side, seed)
-        sysm["side"], sysm["seed"] = side, seed
-        pool.append(sysm)
-    vals = []
-    for k in range(args.warmup + args.steps):
-        cb = cpu_baseline_serve(pool, sample_iters=60)
-        if k >= args.warmup:
-            vals.append(cb["value"])
-    v = float(np.mean(vals))
+    """The reference arm: the reference's own CPU algorithm (the oracle's
+    restatement, no product code loaded) solving the serving request set
+    completely on the host cores. Warm-up steps solve the smallest request;
+    the timed steps solve contiguous groups of requests that together cover
+    the set once."""
+    import oracle
+
+    pool = reference_pool(args.max_side)
+    R = len(pool)
+    smallest = int(np.argmin([p["n"] for p in pool]))
+    for _ in range(args.warmup):
+        reference_solve_requests(pool, [smallest])
+    total_s, lu_s, solved, results = 0.0, 0.0, 0, []
+    for g in step_groups(R, args.steps):
+        dt, dlu, res = reference_solve_requests(pool, g)
+        total_s += dt
+        lu_s += dlu
+        solved += len(g)
+        results += res
+    v = solved / total_s
+    iters = [r["iterations"] for r in results]
+    conv = sum(1 for r in results if r["status"] == oracle.OK)
+    sample = (f"complete solves (LU + PCG) of {solved} requests ({len(set(sum(step_groups(R, args.steps), [])))} "
+              f"distinct of {R}) in {args.steps} steps, {total_s:.1f} s ({lu_s:.2f} s LU), "
+              f"{oracle.num_threads()} threads; stop: {REFERENCE_STOP}")
     return {"metric": METRIC, "impl": "reference", "value": v, "unit": "solves/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": len(pool) / v * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_s / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic 6-DOF lattice systems, seeded",
-            "config": {"workload": f"serve: {len(pool)} requests, lattice side log-uniform [4,64], anisotropy "
-                                   f"10^U(-2,2), relres 1e-8 (the reference's FP32 recursive residual)"},
-            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cb["cores"], "kind": "port",
-                             "sample": cb["sample"]},
+            "config": {"workload": f"serve: {R} requests, lattice side log-uniform [4,64]{side_note(args)}, "
+                                   f"anisotropy 10^U(-2,2), relres 1e-8 on the reference's FP32 recursive residual",
+                       "step": "complete solves of a contiguous group of the requests; the steps cover the set once",
+                       "stop_rule": REFERENCE_STOP},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": oracle.num_threads(), "kind": "port",
+                             "sample": sample},
+            "repo_libraries_loaded": repo_libraries(),
+            "reference_results": {"converged": conv, "of": len(results),
+                                  "iterations_min_median_max": [int(min(iters)), int(np.median(iters)),
+                                                                int(max(iters))]},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -563,6 +634,8 @@ def main():
     ap.add_argument("--side", type=int, default=56, help="kernels workload: lattice side")
     ap.add_argument("--iters", type=int, default=5, help="kernels workload: timed iterations")
     ap.add_argument("--layout", default="auto", choices=["auto", "csr"])
+    ap.add_argument("--max-side", type=int, default=SERVE["side_max"],
+                    help="serve workload: keep only the requests of lattice side <= this (default: all)")
     args = ap.parse_args()
     if args.workload == "kernels":
         world, rank, local = dist_setup()

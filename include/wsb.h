@@ -148,8 +148,11 @@ int wsb_pcg_update_scalars(wsb_context *ctx, wsb_buffer *scalar_results, uint32_
  * static device array of this library (held by every GPU that loads it until
  * exit), which limits n to WSB_NOALLOC_DOT_MAX_N; larger n returns
  * WSB_ERR_BAD_INPUT. The first call on a device resolves that array's
- * address; make it before any stream capture. Calls that overlap on the GPU
- * share the array and race. Enqueued on the context's stream; not waited for. */
+ * address and keeps it for the life of the process; make it before any
+ * stream capture. The kept address assumes the device's primary context is
+ * never torn down (no cudaDeviceReset while the library is in use). Calls
+ * that overlap on the GPU share the array and race. Enqueued on the
+ * context's stream; not waited for. */
 #define WSB_NOALLOC_DOT_MAX_N 16777216u
 int wsb_dot_tree256_noalloc(wsb_context *ctx, const float *d_a, const float *d_b, uint32_t n, float *d_out);
 

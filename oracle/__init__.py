@@ -68,6 +68,11 @@ def lib():
         L.orc_compare_x.argtypes = [C.c_uint64, _f32p, _f32p, _f64p]
         L.orc_compare_x.restype = None
         L.orc_num_threads.restype = C.c_int
+        L.orc_lattice_sizes.argtypes = [C.c_uint32, _u64p]
+        L.orc_lattice_generate.argtypes = [C.c_uint32, C.c_uint64, C.c_double, _u32p, _u32p, _f32p, _u32p, _f32p]
+        _pp = C.POINTER(C.c_void_p)
+        L.orc_pcg_ref_f32_many.argtypes = [C.c_uint32, _u32p, _pp, _pp, _pp, _u32p, _pp, _pp, _pp, _pp,
+                                           C.c_uint64, C.c_float, C.c_float, C.c_uint32, _ip, _u64p]
         _lib = L
     return _lib
 
@@ -202,3 +207,70 @@ def compare_x(x_ref, x):
 
 def num_threads() -> int:
     return lib().orc_num_threads()
+
+
+def lattice_generate(side: int, seed: int = 0, aniso_log10: float = 0.0) -> dict:
+    """The synthetic 6-DOF lattice system of side `side` (row_ptr, col_idx,
+    values, block_starts, b, n, nnz), generated by the oracle's own statement
+    of the generator; bit-identical to the product's wsb_lattice_generate."""
+    sz = np.zeros(3, np.uint64)
+    if lib().orc_lattice_sizes(int(side), _p(sz, _u64p)) != OK:
+        raise ValueError(f"lattice side {side} is too large")
+    n, nnz, nodes = int(sz[0]), int(sz[1]), int(sz[2])
+    rp = np.empty(n + 1, np.uint32)
+    ci = np.empty(nnz, np.uint32)
+    v = np.empty(nnz, np.float32)
+    bs = np.empty(nodes + 1, np.uint32)
+    b = np.empty(n, np.float32)
+    st = lib().orc_lattice_generate(int(side), int(seed), float(aniso_log10), _p(rp, _u32p), _p(ci, _u32p),
+                                    _p(v, _f32p), _p(bs, _u32p), _p(b, _f32p))
+    if st != OK:
+        raise RuntimeError(f"orc_lattice_generate failed with status {st}")
+    return dict(row_ptr=rp, col_idx=ci, values=v, block_starts=bs, b=b, n=n, nnz=nnz)
+
+
+def pcg_ref_f32_many(systems, max_iter, rel_tol, abs_tol=0.0, par_min_n=200_000):
+    """Complete FP32 reference solves (orc_pcg_ref_f32) of many independent
+    systems, each a dict with row_ptr, col_idx, values, block_starts, b and its
+    `lu` (f32[36 nb]); x0 = 0. Systems with n >= par_min_n run one after the
+    other with every host thread inside each solve, the smaller ones
+    concurrently with one thread each. Returns a list of dict(status,
+    iterations, x) in the order given."""
+    cnt = len(systems)
+    order = sorted(range(cnt), key=lambda i: -len(systems[i]["b"]))
+    keep = []  # contiguous arrays that must outlive the call
+
+    def ptr(a, dtype):
+        a = np.ascontiguousarray(a, dtype=dtype)
+        keep.append(a)
+        return a.ctypes.data
+
+    vp = C.c_void_p * cnt
+    n_arr = np.zeros(cnt, np.uint32)
+    nb_arr = np.zeros(cnt, np.uint32)
+    rp, ci, va, lu, bs, bb, xx = vp(), vp(), vp(), vp(), vp(), vp(), vp()
+    xs = []
+    for j, i in enumerate(order):
+        s = systems[i]
+        n = len(s["b"])
+        n_arr[j] = n
+        nb_arr[j] = max(len(s["block_starts"]) - 1, 0)
+        rp[j] = ptr(s["row_ptr"], np.uint32)
+        ci[j] = ptr(s["col_idx"], np.uint32)
+        va[j] = ptr(s["values"], np.float32)
+        lu[j] = ptr(s["lu"], np.float32)
+        bs[j] = ptr(s["block_starts"], np.uint32)
+        bb[j] = ptr(s["b"], np.float32)
+        x = np.zeros(n, np.float32)
+        xs.append(x)
+        xx[j] = x.ctypes.data
+    status = np.zeros(cnt, np.int32)
+    iters = np.zeros(cnt, np.uint64)
+    cast = lambda a: C.cast(a, C.POINTER(C.c_void_p))  # noqa: E731
+    lib().orc_pcg_ref_f32_many(cnt, _p(n_arr, _u32p), cast(rp), cast(ci), cast(va), _p(nb_arr, _u32p), cast(lu),
+                               cast(bs), cast(bb), cast(xx), int(max_iter), np.float32(rel_tol),
+                               np.float32(abs_tol), int(par_min_n), _p(status, _ip), _p(iters, _u64p))
+    out = [None] * cnt
+    for j, i in enumerate(order):
+        out[i] = dict(status=int(status[j]), iterations=int(iters[j]), x=xs[j])
+    return out

@@ -513,6 +513,175 @@ void orc_compare_x(uint64_t n, const float *x_ref, const float *x, double *out)
     out[4] = mx;
 }
 
+/* ------------------------------------------------------------------------- */
+/* Synthetic 6-DOF lattice systems (the measured workloads; not a reference   */
+/* algorithm). An independent C statement of the generator the product ships */
+/* (wsb_lattice_generate), so that the CPU baseline and the reference arm of  */
+/* the benchmark build their inputs without loading the product library. The */
+/* test suite checks the two for bit identity.                               */
+/* Node u = x + L y + L^2 z owns rows 6u..6u+5; every axis-neighbour edge     */
+/* (keyed by its lower node and axis) gets S = (R R^T / 6 + 0.1 I) 10^U(-a,a) */
+/* with R ~ N(0,1) by Box-Muller, assembled as [[S,-S],[-S,S]]; 1e-3 is added */
+/* on the diagonal; b_i ~ U[-1,1). FP64 accumulation, one rounding to f32.     */
+/* ------------------------------------------------------------------------- */
+#define ORC_GOLDEN 0x9E3779B97F4A7C15ull
+
+static uint64_t orc_fin64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+/* Counter-based stream keyed by (seed, key). */
+static uint64_t orc_stream_init(uint64_t seed, uint64_t key)
+{
+    return orc_fin64((seed ^ orc_fin64(key * 0xD1B54A32D192ED03ull + 1 + ORC_GOLDEN)) + ORC_GOLDEN);
+}
+
+static double orc_stream_uniform(uint64_t *state) /* [0, 1) */
+{
+    *state += ORC_GOLDEN;
+    return (double)(orc_fin64(*state) >> 11) * 0x1.0p-53;
+}
+
+static void orc_edge_stiffness(uint64_t seed, uint64_t key, double aniso, double S[36])
+{
+    uint64_t st = orc_stream_init(seed, key);
+    double R[36];
+    for (int k = 0; k < 36; k += 2) {
+        double u1 = 1.0 - orc_stream_uniform(&st);
+        double u2 = orc_stream_uniform(&st);
+        double rad = sqrt(-2.0 * log(u1));
+        R[k] = rad * cos(6.283185307179586 * u2);
+        R[k + 1] = rad * sin(6.283185307179586 * u2);
+    }
+    double scale = 1.0;
+    if (aniso > 0.0) scale = pow(10.0, (2.0 * orc_stream_uniform(&st) - 1.0) * aniso);
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) {
+            double dotp = 0.0;
+            for (int k = 0; k < 6; ++k) dotp += R[i * 6 + k] * R[j * 6 + k];
+            S[i * 6 + j] = (dotp / 6.0 + (i == j ? 0.1 : 0.0)) * scale;
+        }
+}
+
+/* Axis neighbours of node u including itself, ascending index order
+ * (-z, -y, -x, self, +x, +y, +z). axis -1 marks the node itself; lower = 1
+ * when the neighbour is the edge's lower node. Returns the count. */
+static int orc_lattice_nbrs(int64_t u, int64_t L, int64_t *w, int *axis, int *lower)
+{
+    const int64_t LL = L * L, x = u % L, y = (u / L) % L, z = u / LL;
+    int c = 0;
+#define ORC_NB(cond, node, ax, lo) if (cond) { w[c] = (node); axis[c] = (ax); lower[c] = (lo); ++c; }
+    ORC_NB(z > 0, u - LL, 2, 1)
+    ORC_NB(y > 0, u - L, 1, 1)
+    ORC_NB(x > 0, u - 1, 0, 1)
+    ORC_NB(1, u, -1, 0)
+    ORC_NB(x + 1 < L, u + 1, 0, 0)
+    ORC_NB(y + 1 < L, u + L, 1, 0)
+    ORC_NB(z + 1 < L, u + LL, 2, 0)
+#undef ORC_NB
+    return c;
+}
+
+/* Sizes of the side-L lattice system: out[0] = n, out[1] = nnz, out[2] = nodes. */
+int orc_lattice_sizes(uint32_t L, uint64_t *out)
+{
+    uint64_t l = L, nodes = l * l * l, edges = l >= 1 ? 3 * l * l * (l - 1) : 0;
+    out[0] = 6 * nodes;
+    out[1] = 36 * (nodes + 2 * edges);
+    out[2] = nodes;
+    return (out[0] > 0xffffffffull || out[1] > 0xffffffffull) ? ORC_BAD_INPUT : ORC_OK;
+}
+
+int orc_lattice_generate(uint32_t L, uint64_t seed, double aniso, uint32_t *row_ptr, uint32_t *col,
+                         float *val, uint32_t *bs, float *b)
+{
+    uint64_t sz[3];
+    if (orc_lattice_sizes(L, sz) != ORC_OK) return ORC_BAD_INPUT;
+    const int64_t nodes = (int64_t)sz[2];
+    /* First entry of each node's rows: 36 per neighbour (self included). */
+    uint64_t *node_off = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(nodes + 1));
+    if (!node_off) return ORC_NO_MEMORY;
+    node_off[0] = 0;
+    for (int64_t u = 0; u < nodes; ++u) {
+        int64_t w[7];
+        int ax[7], lo[7];
+        node_off[u + 1] = node_off[u] + 36ull * (uint64_t)orc_lattice_nbrs(u, L, w, ax, lo);
+    }
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t u = 0; u < nodes; ++u) {
+        int64_t w[7];
+        int ax[7], lo[7];
+        const int c = orc_lattice_nbrs(u, L, w, ax, lo);
+        double blk[7][36], diag[36];
+        memset(diag, 0, sizeof diag);
+        int self = 0;
+        for (int k = 0; k < c; ++k) {
+            if (ax[k] < 0) {
+                self = k;
+                continue;
+            }
+            const int64_t low = lo[k] ? w[k] : u;
+            double S[36];
+            orc_edge_stiffness(seed, (uint64_t)low * 3 + (uint64_t)ax[k] + 1, aniso, S);
+            for (int q = 0; q < 36; ++q) {
+                blk[k][q] = -S[q];
+                diag[q] += S[q];
+            }
+        }
+        for (int i = 0; i < 6; ++i) diag[i * 6 + i] += 1e-3;
+        memcpy(blk[self], diag, sizeof diag);
+        for (int a = 0; a < 6; ++a) {
+            const uint64_t row = 6 * (uint64_t)u + (uint64_t)a;
+            uint64_t k0 = node_off[u] + (uint64_t)a * 6 * (uint64_t)c;
+            row_ptr[row] = (uint32_t)k0;
+            for (int k = 0; k < c; ++k)
+                for (int j = 0; j < 6; ++j, ++k0) {
+                    col[k0] = (uint32_t)(6 * w[k] + j);
+                    val[k0] = (float)blk[k][a * 6 + j];
+                }
+            uint64_t sb = orc_stream_init(seed, 0x4000000000000000ull + row);
+            b[row] = (float)(2.0 * orc_stream_uniform(&sb) - 1.0);
+        }
+        bs[u] = (uint32_t)(6 * u);
+    }
+    row_ptr[sz[0]] = (uint32_t)node_off[nodes];
+    bs[nodes] = (uint32_t)sz[0];
+    free(node_off);
+    return ORC_OK;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Many independent FP32 reference solves (orc_pcg_ref_f32 each), for the    */
+/* timed CPU baseline: systems with n >= par_min_n run one after another with */
+/* every host thread inside each solve; the smaller ones run concurrently,   */
+/* one thread each (the inner loops stay serial below ORC_PAR_MIN rows, and  */
+/* nested parallel regions are off; callers list the systems largest first */
+/* so that the dynamic schedule balances). Per-system status and iteration   */
+/* counts out; x[i] receives the solution of system i.                       */
+/* ------------------------------------------------------------------------- */
+int orc_pcg_ref_f32_many(uint32_t count, const uint32_t *n, const uint32_t *const *row_ptr,
+                         const uint32_t *const *col, const float *const *val, const uint32_t *nb,
+                         const float *const *lu, const uint32_t *const *bs, const float *const *b,
+                         float *const *x, uint64_t max_iter, float rel_tol, float abs_tol, uint32_t par_min_n,
+                         int *status, uint64_t *iters)
+{
+    for (uint32_t i = 0; i < count; ++i)
+        if (n[i] >= par_min_n)
+            status[i] = orc_pcg_ref_f32(n[i], row_ptr[i], col[i], val[i], nb[i], lu[i], bs[i], b[i], x[i],
+                                        max_iter, rel_tol, abs_tol, &iters[i], NULL, NULL);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t j = 0; j < (int64_t)count; ++j) {
+        const uint32_t i = (uint32_t)j;
+        if (n[i] < par_min_n)
+            status[i] = orc_pcg_ref_f32(n[i], row_ptr[i], col[i], val[i], nb[i], lu[i], bs[i], b[i], x[i],
+                                        max_iter, rel_tol, abs_tol, &iters[i], NULL, NULL);
+    }
+    return ORC_OK;
+}
+
 int orc_num_threads(void)
 {
 #ifdef _OPENMP

@@ -75,14 +75,20 @@ def test_reference_arm_line_on_one_rank():
     # The reference arm runs on host cores only: its JSON line carries the
     # contract's keys, the CPU baseline it measured and a zero-copy e2e.
     env = {k: v for k, v in os.environ.items() if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE")}
-    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "0"], env=env, capture_output=True, text=True, timeout=600)
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "3",
+                        "--warmup", "1", "--max-side", "8"], env=env, capture_output=True, text=True, timeout=600)
     assert p.returncode == 0, p.stderr
     lines = [ln for ln in p.stdout.splitlines() if ln.strip()]
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["metric"] == bench.METRIC and d["unit"] == "solves/s"
-    assert d["higher_is_better"] is True and d["n_gpus"] == 1 and d["steps"] == 1
+    assert d["higher_is_better"] is True and d["n_gpus"] == 1 and d["steps"] == 3
     assert d["value"] > 0 and d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["kind"] == "port"
     assert d["cpu_baseline"]["cores"] >= 1
+    # Complete solves of every request of the (reduced) set, not a projection.
+    n_req = len(bench.serve_set(8))
+    assert d["reference_results"] == {**d["reference_results"], "converged": n_req, "of": n_req}
+    assert "complete solves" in d["cpu_baseline"]["sample"]
+    # The reference process maps the oracle and never the product library.
+    assert d["repo_libraries_loaded"] == ["oracle/liboracle.so"]
     assert d["e2e"] == {"value": d["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}

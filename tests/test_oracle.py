@@ -112,3 +112,36 @@ def test_lu_zero_pivot_and_identity_padding():
     assert st == 0
     m = lu.reshape(6, 6)
     assert np.array_equal(np.diag(m), np.array([2, 4, 8, 1, 1, 1], np.float32))
+
+
+@pytest.mark.parametrize("side,seed,aniso", [(1, 3, 0.0), (4, 7, 2.0), (7, 11, 3.0), (10, 2024, 0.0)])
+def test_oracle_lattice_generator_matches_the_product_generator(side, seed, aniso):
+    # The benchmark's CPU legs build their inputs with the oracle's generator
+    # (so that they never load the product library); both must give the same
+    # systems bit for bit.
+    import wgpu_solver_backend_b200 as wsb
+
+    a = oracle.lattice_generate(side, seed, aniso)
+    b = wsb.lattice_generate(side, seed=seed, aniso_log10=aniso)
+    assert a["n"] == b["n"] and a["nnz"] == b["nnz"]
+    for k in ("row_ptr", "col_idx", "values", "block_starts", "b"):
+        assert np.array_equal(a[k].view(np.uint32), b[k].view(np.uint32)), k
+
+
+def test_many_reference_solves_equal_single_solves():
+    # The batched CPU baseline runs orc_pcg_ref_f32 per system, concurrently
+    # for small systems and with inner threads for large ones: same bits as
+    # one solve at a time.
+    systems = []
+    for side, seed in ((3, 1), (5, 2), (4, 3), (6, 4)):
+        s = oracle.lattice_generate(side, seed, 1.0)
+        st, lu, _, _ = oracle.build_lu_blocks_6(s["n"], s["row_ptr"], s["col_idx"], s["values"], s["block_starts"])
+        assert st == oracle.OK
+        systems.append(dict(s, lu=lu))
+    many = oracle.pcg_ref_f32_many(systems, 5000, 1e-6, 0.0, par_min_n=500)
+    for s, m in zip(systems, many):
+        one = oracle.pcg_ref_f32(s["row_ptr"], s["col_idx"], s["values"], s["lu"], s["block_starts"], s["b"],
+                                 np.zeros(s["n"], np.float32), 5000, 1e-6, 0.0)
+        assert m["status"] == one["status"] == oracle.OK
+        assert m["iterations"] == one["iterations"]
+        assert np.array_equal(m["x"].view(np.uint32), one["x"].view(np.uint32))

@@ -739,7 +739,7 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
     if (h_sp_rb_->error) {
         // A bounded wait ran out inside a kernel: end every system in flight.
         const uint32_t code = h_sp_rb_->error;
-        const int rc2 = (code & 7u) ? fail(ctx_, WSB_ERR_TIMEOUT, "a device wait ran out (kernel code %u)", code)
+        const int rc2 = (code & kErrWaitMask) ? fail(ctx_, WSB_ERR_TIMEOUT, "a device wait ran out (kernel code %u)", code)
                                     : fail(ctx_, WSB_ERR_CUDA, "a kernel met an invalid work item (code %u)", code);
         for (uint32_t s2 = 0; s2 < slots_.size(); ++s2)
             if (slots_[s2] && slots_[s2]->phase == Slot::RUNNING) finish_slot(s2, rc2);
@@ -798,7 +798,7 @@ int Engine::profile_kernels(uint32_t s, uint32_t iters, double ms[5]) {
     WSB_CUDA_TRY(ctx_, cudaGetLastError());
     WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(h_sp_rb_, d_sp_, sizeof(StepParams), cudaMemcpyDeviceToHost, stream_));
     WSB_CUDA_TRY(ctx_, cudaStreamSynchronize(stream_));
-    if (h_sp_rb_->error) return fail(ctx_, (h_sp_rb_->error & 7u) ? WSB_ERR_TIMEOUT : WSB_ERR_CUDA,
+    if (h_sp_rb_->error) return fail(ctx_, (h_sp_rb_->error & kErrWaitMask) ? WSB_ERR_TIMEOUT : WSB_ERR_CUDA,
                                      "kernel error code %u during profiling", h_sp_rb_->error);
     double acc[3] = {0, 0, 0};
     for (uint32_t i = 0; i < iters; ++i)

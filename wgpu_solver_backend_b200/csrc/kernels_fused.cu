@@ -323,7 +323,7 @@ __device__ __forceinline__ bool check_spmv(const SysDesc *__restrict__ sys, cons
         return true;
     }
     if (it->sys >= sp->num_sys || it->tile >= sys[it->sys].n_stiles) {
-        atomicOr(const_cast<uint32_t *>(&sp->error), 8u);  // invalid work item: skipped
+        atomicOr(const_cast<uint32_t *>(&sp->error), kErrBadItem);  // invalid work item: skipped
         return false;
     }
     return !(kMode == M_LOOP && !sys[it->sys].st->active);
@@ -611,7 +611,7 @@ __device__ __forceinline__ void spmv_producer(const SysDesc *__restrict__ sys, S
             for (uint32_t i = 0; i < n_out; ++i) {
                 const uint32_t s = k % NS;
                 if (k >= NS && !mbar_wait(&empty[s], ((k / NS) - 1) & 1u)) {
-                    atomicOr(&sp->error, 16u);
+                    atomicOr(&sp->error, kErrSpmvProducerWait);
                     err = true;
                     break;
                 }
@@ -656,7 +656,7 @@ __device__ __forceinline__ void spmv_gatherer(const SysDesc *__restrict__ sys, S
         if (lane == 0) ok = mbar_wait(&meta[s], par) ? 1u : 0u;
         ok = __shfl_sync(0xffffffffu, ok, 0);
         if (!ok) {
-            if (lane == 0) atomicOr(&sp->error, 64u);
+            if (lane == 0) atomicOr(&sp->error, kErrGatherWait);
             break;
         }
         mbar_wait(&meta[s], par);  // completed: the descriptor is visible
@@ -711,7 +711,7 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
         if (tid == 0) s_ok[k & 1u] = (mbar_wait(&gath[s], par) && mbar_wait(&full[s], par)) ? 1 : 0;
         csync<NC>();
         if (!s_ok[k & 1u]) {
-            if (tid == 0) atomicOr(&sp->error, 1u);
+            if (tid == 0) atomicOr(&sp->error, kErrSpmvConsumerWait);
             return;
         }
         mbar_observe(&gath[s], par);
@@ -810,7 +810,7 @@ __device__ __forceinline__ bool check_upd(const SysDesc *__restrict__ sys, const
                                           uint32_t nw, WorkItem it) {
     if (idx >= nw) return false;
     if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_utiles) {
-        atomicOr(const_cast<uint32_t *>(&sp->error), 8u);  // invalid work item: skipped
+        atomicOr(const_cast<uint32_t *>(&sp->error), kErrBadItem);  // invalid work item: skipped
         return false;
     }
     return kInit || sys[it.sys].st->active;
@@ -1082,7 +1082,7 @@ __device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, St
             for (uint32_t i = 0; i < n_out; ++i) {
                 const uint32_t s = k % NS;
                 if (k >= NS && !mbar_wait(&empty[s], ((k / NS) - 1) & 1u)) {
-                    atomicOr(&sp->error, 32u);
+                    atomicOr(&sp->error, kErrUpdProducerWait);
                     err = true;
                     break;
                 }
@@ -1144,7 +1144,7 @@ __device__ __forceinline__ void upd_consumers(const SysDesc *__restrict__ sys, S
         if (lt == 0) g.s_ok[n & 1u] = mbar_wait(&full[s], par) ? 1 : 0;
         gsync<GT, BAR>();
         if (!g.s_ok[n & 1u]) {
-            if (lt == 0) atomicOr(&sp->error, kInit ? 4u : 2u);
+            if (lt == 0) atomicOr(&sp->error, kInit ? kErrInitConsumerWait : kErrUpdConsumerWait);
             return;
         }
         mbar_observe(&full[s], par);
@@ -1299,7 +1299,7 @@ __global__ void __launch_bounds__(kThreads) k_pupdate(const SysDesc *__restrict_
     for (uint32_t w = blockIdx.x; w < nw; w += gridDim.x) {
         const WorkItem it = work[w];
         if (it.sys >= sp->num_sys || it.tile * (uint32_t)kChunkRows >= sys[it.sys].n) {
-            if (threadIdx.x == 0) atomicOr(&sp->error, 8u);
+            if (threadIdx.x == 0) atomicOr(&sp->error, kErrBadItem);
             continue;
         }
         const SysDesc &S = sys[it.sys];
@@ -1372,7 +1372,7 @@ __global__ void __launch_bounds__(kThreads) k_resid64(const SysDesc *__restrict_
     for (uint32_t w = blockIdx.x; w < nw; w += gridDim.x) {
         const WorkItem it = work[w];
         if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_utiles) {
-            if (threadIdx.x == 0) atomicOr(&sp->error, 8u);
+            if (threadIdx.x == 0) atomicOr(&sp->error, kErrBadItem);
             continue;
         }
         const SysDesc &S = sys[it.sys];
@@ -1428,7 +1428,7 @@ __global__ void __launch_bounds__(kThreads) k_refine(const SysDesc *__restrict__
     for (uint32_t w = blockIdx.x; w < nw; w += gridDim.x) {
         const WorkItem it = work[w];
         if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_utiles) {
-            if (threadIdx.x == 0) atomicOr(&sp->error, 8u);
+            if (threadIdx.x == 0) atomicOr(&sp->error, kErrBadItem);
             continue;
         }
         const SysDesc &S = sys[it.sys];
@@ -1448,7 +1448,7 @@ __global__ void __launch_bounds__(kThreads) k_x64_to_x32(const SysDesc *__restri
     for (uint32_t w = blockIdx.x; w < nw; w += gridDim.x) {
         const WorkItem it = work[w];
         if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_utiles) {
-            if (threadIdx.x == 0) atomicOr(&sp->error, 8u);
+            if (threadIdx.x == 0) atomicOr(&sp->error, kErrBadItem);
             continue;
         }
         const SysDesc &S = sys[it.sys];

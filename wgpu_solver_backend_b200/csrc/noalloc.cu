@@ -25,7 +25,10 @@ static __device__ __align__(256) float g_dot_scratch[kScratchFloats];
 
 // Device address of g_dot_scratch per device. In host code the symbol is
 // only a stand-in; cudaGetSymbolAddress with the device current gives the
-// address a kernel can use.
+// address a kernel can use. It is looked up once per device and kept for the
+// life of the process, which assumes the device's primary context (and with
+// it this module's copy of the array) is never reset while the library is in
+// use: after a cudaDeviceReset the kept address would be stale.
 std::mutex g_mu;
 float *g_addr[64] = {};
 

@@ -122,6 +122,20 @@ struct SysDesc {
     double *history;                   // hist_cap entries or null
 };
 
+// Bits of StepParams::error. The wait bits mean a bounded mbarrier wait ran
+// out (the kernel recorded the bit, drained its own copies and returned); the
+// host reports them as WSB_ERR_TIMEOUT. kErrBadItem marks a work item that
+// names a system or tile that does not exist (the item was skipped).
+constexpr uint32_t kErrSpmvConsumerWait = 1u;   // SpMV consumers: stage data
+constexpr uint32_t kErrUpdConsumerWait = 2u;    // update consumers (loop kernel)
+constexpr uint32_t kErrInitConsumerWait = 4u;   // update consumers (init kernel)
+constexpr uint32_t kErrBadItem = 8u;            // invalid work item
+constexpr uint32_t kErrSpmvProducerWait = 16u;  // SpMV producer: a free stage
+constexpr uint32_t kErrUpdProducerWait = 32u;   // update producer: a free stage
+constexpr uint32_t kErrGatherWait = 64u;        // SpMV gather warp: a tile descriptor
+constexpr uint32_t kErrWaitMask = kErrSpmvConsumerWait | kErrUpdConsumerWait | kErrInitConsumerWait |
+                                  kErrSpmvProducerWait | kErrUpdProducerWait | kErrGatherWait;
+
 // Kernel parameters of one loop step that the host may change between graph
 // launches (work lists, counts); lives in device memory so a captured graph
 // stays valid.
