@@ -301,9 +301,10 @@ def mixed_kw():
                 target_relres=SERVE["target"], inner_rel_tol=SERVE["inner"])
 
 
-def served_pass(srv, pool, arrivals=None):
+def served_pass(srv, pool, arrivals=None, targets=None):
     """Submits every request (at its arrival time, or all at once), waits for
-    all. Returns (makespan_s, latencies_ms, results)."""
+    all. targets: per-request FP64 relative residual (default: the set's).
+    Returns (makespan_s, latencies_ms, results)."""
     kw = mixed_kw()
     t0 = time.perf_counter()
     rids = []
@@ -312,6 +313,8 @@ def served_pass(srv, pool, arrivals=None):
             dt = t0 + arrivals[i] - time.perf_counter()
             if dt > 0:
                 time.sleep(dt)
+        if targets is not None:
+            kw["target_relres"] = float(targets[i])
         rids.append(srv.submit(s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], s["b"], **kw))
     res = [srv.wait(r, 600.0) for r in rids]
     mk = time.perf_counter() - t0
@@ -405,6 +408,101 @@ def cpu_baseline_serve(pool, stride=4):
                       f"converged; stop: {REFERENCE_STOP}"}
 
 
+def kernel_block(kt, info, n, peak):
+    """Per-kernel mean launch time, algorithmic bytes, GB/s and fraction of
+    the HBM peak for the three loop kernels of one matrix."""
+    out = {}
+    for k, b in (("spmv", info["spmv_bytes"]), ("update", 28 * n + 144 * info["num_blocks"]), ("pupdate", 12 * n)):
+        ms = kt[k + "_ms"]
+        out[k] = {"us": ms * 1e3, "bytes": int(b), "gbs": b / ms / 1e6, "frac": b / ms / 1e6 / peak}
+    return out
+
+
+def measure_c2(ctx, stream, peak):
+    """The plain 80^3 system (n = 3,072,000, nnz = 127,641,600, tolerance
+    1e-6) in both layouts: per-kernel times of the loop kernels (CUDA events
+    per launch), whole solves (CUDA events, graph loop), per-iteration GB/s."""
+    import torch
+
+    import wgpu_solver_backend_b200 as wsb
+
+    s = wsb.lattice_generate(PLAIN["side"], seed=PLAIN["seed"])
+    n = s["n"]
+    d_b = torch.from_numpy(s["b"]).cuda()
+    d_x = torch.zeros(n, dtype=torch.float32, device="cuda")
+    kw = dict(max_iter=PLAIN["max_iter"], rel_tol=PLAIN["rel_tol"])
+    out = {"workload": "plain 80^3 lattice, n=3072000, nnz=127641600, b ~ U[-1,1], rel tol 1e-6"}
+    for name, layout in (("bsr6", wsb.LAYOUT_BSR6), ("csr", wsb.LAYOUT_CSR)):
+        m = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], layout=layout)
+        info = m.info
+        torch.cuda.synchronize()
+        kt = m.kernel_times(d_b.data_ptr(), iterations=20)
+        d_x.zero_()
+        m.solve_device(d_b.data_ptr(), d_x.data_ptr(), **kw)  # warm-up
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps, ms = 3, 0.0
+        for _ in range(reps):
+            d_x.zero_()
+            torch.cuda.synchronize()
+            e0.record(stream)
+            r = m.solve_device(d_b.data_ptr(), d_x.data_ptr(), **kw)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1) / reps
+        it = int(r["iterations"])
+        ib = info["iteration_bytes"]
+        out[name] = {"kernels": kernel_block(kt, info, n, peak), "solve_ms": ms, "iterations": it,
+                     "iteration_us": ms * 1e3 / it, "iteration_bytes": int(ib),
+                     "iteration_gbs": ib * it / (ms / 1e3) / 1e9, "iteration_frac": ib * it / (ms / 1e3) / 1e9 / peak,
+                     "matrix_bytes": int(info["device_bytes"])}
+        del m
+    return out
+
+
+C4 = dict(systems=512, side_min=4, side_max=24, seed=512, rel_tol=1e-8, max_iter=20000)
+
+
+def measure_c4(ctx, stream, peak):
+    """512 independent systems (lattice side uniform in 4..24, own seeds and
+    right-hand sides), tolerance 1e-8 with FP64 reductions, one batched
+    solve (persistent kernels, graph loop, retire in place). Reports
+    solves/s and the batch's algorithmic bytes (sum over systems of
+    iterations x bytes per iteration) against the HBM peak."""
+    import torch
+
+    import wgpu_solver_backend_b200 as wsb
+
+    rng = np.random.default_rng(C4["seed"])
+    sides = rng.integers(C4["side_min"], C4["side_max"] + 1, C4["systems"])
+    systems = [wsb.lattice_generate(int(sd), seed=50_000 + i) for i, sd in enumerate(sides)]
+    mats = [wsb.Matrix.create(ctx, q["row_ptr"], q["col_idx"], q["values"], q["block_starts"]) for q in systems]
+    kw = dict(max_iter=C4["max_iter"], rel_tol=C4["rel_tol"])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times, res = [], None
+    for rep in range(3):  # the first is a warm-up
+        bt = wsb.Batch(ctx)
+        for m, q in zip(mats, systems):
+            bt.add(m, q["b"], **kw)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        bt.solve()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if rep:
+            times.append(e0.elapsed_time(e1) / 1e3)
+        res = [bt.result(i, q["n"])[1] for i, q in enumerate(systems)]
+        del bt
+    t = float(np.mean(times))
+    iters = [int(r["iterations"]) for r in res]
+    byts = sum(it * m.info["iteration_bytes"] for it, m in zip(iters, mats))
+    return {"workload": f"{C4['systems']} systems, lattice side uniform {C4['side_min']}..{C4['side_max']} "
+                        f"({sum(q['n'] for q in systems)} unknowns), rel tol 1e-8, FP64 reductions, one batch",
+            "solves_per_s": C4["systems"] / t, "batch_ms": t * 1e3,
+            "converged": sum(1 for r in res if r["rc"] == 0), "of": len(res),
+            "iterations_min_median_max": [min(iters), int(np.median(iters)), max(iters)],
+            "algorithmic_bytes": int(byts), "gbs": byts / t / 1e9, "frac": byts / t / 1e9 / peak}
+
+
 def run_serve(args, world, rank, local):
     import torch
 
@@ -451,6 +549,11 @@ def run_serve(args, world, rank, local):
     rng = np.random.default_rng(11)
     arrivals = np.cumsum(rng.exponential(1.0 / lam, R)) - 0.0
     mk_p, lat_p, _ = served_pass(srv, pool, arrivals)
+    # The tolerance mix of the serving configuration: each request's target
+    # FP64 relative residual is 1e-6 or 1e-10 with probability 1/2.
+    tmix = np.where(np.random.default_rng(13).random(R) < 0.5, 1e-6, 1e-10)
+    mk_mix, lat_mix, res_mix = served_pass(srv, pool, targets=tmix)
+    mix_ok = sum(1 for r, tg in zip(res_mix, tmix) if r["rc"] == 0 and r["final_relres"] <= tg)
     st = srv.stats()
     srv.close()
     # Resident batch: matrices already in HBM, one batched solve of the set.
@@ -467,8 +570,10 @@ def run_serve(args, world, rank, local):
         e1.record(stream)
         torch.cuda.synchronize()
         dev_s += e0.elapsed_time(e1) / 1e3
+        pass_bytes = 0
         for i, p in enumerate(pool):
             _, r = bt.result(i, p["n"])
+            pass_bytes += int(r["iterations"]) * mats[i].info["iteration_bytes"]
             if i == 0:
                 batch_launches += r["kernel_launches"]
             if r["rc"] != 0:
@@ -476,6 +581,7 @@ def run_serve(args, world, rank, local):
                                  "iterations": r["iterations"], "sweeps": r["refine_sweeps"],
                                  "relres": r["final_relres"], "breakdown": r["breakdown_kind"]})
         del bt
+    pass_s = dev_s / args.steps
     dev_s = reduce_max(dev_s, world)
     # Plain baseline: the same requests one at a time (host arrays, matrix
     # upload and LU per request, then the solve), as a plain per-solve GPU PCG.
@@ -507,8 +613,10 @@ def run_serve(args, world, rank, local):
     kt = mats[big].kernel_times(d_b.data_ptr(), iterations=10)
     info = mats[big].info
     peak, peak_kind = peaks()
-    spmv_gbs = info["spmv_bytes"] / (kt["spmv_ms"] / 1e3) / 1e9
-    upd_bytes = 28 * pool[big]["n"] + 144 * info["num_blocks"]
+    serve_largest = kernel_block(kt, info, pool[big]["n"], peak)
+    c2 = measure_c2(ctx, stream, peak)
+    c4 = measure_c4(ctx, stream, peak)
+    top = c2["bsr6"]["kernels"]["spmv"]
     e2e = replica_rate(world, args.steps * R, e2e_s)
     line = {
         "metric": METRIC, "value": replica_rate(world, args.steps * R, dev_s), "unit": "solves/s", "n_gpus": world,
@@ -534,12 +642,22 @@ def run_serve(args, world, rank, local):
                              (world * R / plain_res_s)},
         "results": {"ok": ok, "of": len(results), "max_final_relres": relres_max,
                     "iterations_min_median_max": [int(min(iters)), int(np.median(iters)), int(max(iters))]},
-        "roofline": {"bound": "hbm", "kernel": "k_spmv_loop (SpMV + p.Ap), largest system of the set",
-                     "achieved": spmv_gbs, "peak": peak, "unit": "GB/s", "frac": spmv_gbs / peak,
-                     "peak_kind": peak_kind, **spmv_traffic(info["spmv_bytes"]),
-                     "algorithmic_bytes_per_launch": info["spmv_bytes"],
-                     "launch_us": kt["spmv_ms"] * 1e3,
-                     "update_kernel_gbs": upd_bytes / kt["update_ms"] / 1e6},
+        "roofline": {"bound": "hbm", "kernel": "k_spmv_loop (SpMV + p.Ap) on the 3.07M-unknown 80^3 system, BSR6 "
+                               "(the layout the library picks for it); CSR beside it in c2",
+                     "achieved": top["gbs"], "peak": peak, "unit": "GB/s", "frac": top["frac"],
+                     "peak_kind": peak_kind, **spmv_traffic(top["bytes"]),
+                     "algorithmic_bytes_per_launch": top["bytes"], "launch_us": top["us"]},
+        "resident_pass_hbm": {"algorithmic_bytes": pass_bytes, "gbs": pass_bytes / pass_s / 1e9,
+                              "frac": pass_bytes / pass_s / 1e9 / peak,
+                              "note": "sum over requests of PCG iterations x bytes per iteration; the FP64 "
+                                      "refinement sweeps' residual and update passes are not counted"},
+        "c2": c2,
+        "c4": c4,
+        "serve_largest_system_kernels": serve_largest,
+        "serve_tolerance_mix": {"targets": "FP64 relres 1e-6 or 1e-10, p = 1/2 each (seeded)",
+                                "solves_per_s": R / mk_mix, "met_target": mix_ok, "of": R,
+                                "p50_ms": float(np.percentile(lat_mix, 50)), "p99_ms": float(np.percentile(lat_mix, 99)),
+                                "path": "continuous-batching server, burst, host arrays"},
         "server": {"steps": st["steps"], "device_bytes_peak": st["device_bytes_peak"]},
         "failures": failures[:20],
         "host_generate_s": t_gen,

@@ -73,6 +73,13 @@ int wsb_context_adapter_info(const wsb_context *ctx, wsb_adapter_info *out);
  * (passed as void*); NULL restores the context's own stream. */
 int wsb_context_set_stream(wsb_context *ctx, void *cuda_stream);
 int wsb_context_synchronize(wsb_context *ctx);
+/* Failure detection (no counterpart in the reference, which blocks on
+ * futures without a limit): every wait of the pipelined solver kernels gives
+ * up after `cycles` SM clock cycles (0 restores the default of about 2 s);
+ * the kernel then records the wait, drains its own copies in flight and
+ * returns, and the solve reports WSB_ERR_TIMEOUT for every system in flight.
+ * Applies to solves, batches and servers started on this context afterwards. */
+int wsb_context_set_wait_limit(wsb_context *ctx, uint64_t cycles);
 
 /* ------------------------------------------------------------------------- */
 /* Device buffers (GpuBuffer<T>, gpu/buffer.rs:6-17)                          */
@@ -287,8 +294,20 @@ int wsb_solve(wsb_context *ctx, wsb_matrix *m, const float *b, float *x, uint64_
 /* Same with device pointers (d_b: n floats, d_x: n floats in/out). */
 int wsb_solve_device(wsb_context *ctx, wsb_matrix *m, const float *d_b, float *d_x, uint64_t max_iter,
                      float rel_tol, float abs_tol, const wsb_solve_opts *opts, wsb_solve_result *result);
-/* y = A x with the product SpMV kernel of the matrix's layout (device pointers). */
+/* y = A x with the product SpMV kernel of the matrix's layout (device
+ * pointers), as SpmvExecutor::encode_spmv does for its own buffers
+ * (spmv_exec.rs:120-147). Enqueued on the context's stream, not waited for.
+ * The kernel's descriptor and error word belong to the matrix; a kernel error
+ * (a device wait that ran out) is reported by a later wsb_matrix_spmv_device
+ * call on the matrix once its read-back has completed, or by
+ * wsb_matrix_spmv_check. Calls on one matrix from several streams share the
+ * descriptor and the error word. */
 int wsb_matrix_spmv_device(wsb_context *ctx, wsb_matrix *m, const float *d_x, float *d_y);
+/* Waits for the last wsb_matrix_spmv_device launch on m and returns the
+ * status of the launches since the last reported error (WSB_OK, or
+ * WSB_ERR_TIMEOUT / WSB_ERR_CUDA with wsb_last_error). No counterpart in the
+ * reference, whose SpMV executor blocks on every submission. */
+int wsb_matrix_spmv_check(wsb_context *ctx, wsb_matrix *m);
 
 /* Measurement aid (no counterpart in the reference): runs `iterations` PCG
  * iterations of this matrix with right-hand side d_b (device) outside the
@@ -318,20 +337,33 @@ void wsb_batch_destroy(wsb_batch *bt);
 /* Serving: continuous batching of solve requests                            */
 /* ------------------------------------------------------------------------- */
 typedef struct wsb_server wsb_server;
+/* wsb_server_opts.flags */
+#define WSB_SERVER_BORROW_INPUTS 1u /* submit does not copy: the caller's arrays (row_ptr, col_idx,
+                                       values, block_starts, b, x0) are read in place and must stay
+                                       valid and unchanged until poll/wait reports the request done */
+#define WSB_SERVER_DEVICE_PREP 2u   /* the column check, BSR6 conversion and block LU of each request
+                                       run on the GPU (as wsb_matrix_create does) instead of the
+                                       uploader threads' host builders */
 typedef struct wsb_server_opts {
     uint32_t struct_size;
     uint32_t max_active;          /* systems iterated together (0: no limit) */
     uint64_t memory_budget_bytes; /* device bytes for resident systems (0: 120 GB) */
-    uint32_t iters_per_step;      /* PCG iterations between scheduler steps (0: 16) */
-    uint32_t reserved;
+    uint32_t iters_per_step;      /* PCG iterations between scheduler steps while requests are still
+                                     arriving (0: 16); 4x that when none is on its way */
+    uint32_t flags;               /* WSB_SERVER_* above */
 } wsb_server_opts;
 typedef struct wsb_server_stats {
     uint64_t submitted, completed, failed, rejected;
     uint64_t active, pending;
     uint64_t steps;
     uint64_t device_bytes_in_use, device_bytes_peak;
-    double busy_ms;
+    double busy_ms;             /* scheduler: time inside engine steps (graph launch to state read-back) */
     uint64_t kernel_launches;   /* kernels the scheduler has launched so far */
+    double host_prep_ms;        /* uploaders: host validation and LU (summed over threads) */
+    double upload_ms;           /* uploaders: copies and device-side preparation (summed over threads) */
+    double admit_ms;            /* scheduler: adding ready requests to the engine (b, x0 uploads) */
+    double retire_ms;           /* scheduler: reading results back and releasing finished requests */
+    double sched_idle_ms;       /* scheduler: waiting for work */
 } wsb_server_stats;
 
 int wsb_server_create(wsb_context *ctx, const wsb_server_opts *opts, wsb_server **out);

@@ -1,7 +1,7 @@
 """Generate the golden fixtures under tests/golden/ from the reference's datasets.
 
-Run in a container where the reference repository is mounted (default
-/root/reference); the GPU tests only read the committed outputs.
+Run where a checkout of the reference repository is available and pass its
+root with --reference; the GPU tests only read the committed outputs.
 
 For each of datasets/pcg_block_jacobi_dataset_{1,2,3}.txt this script
 1. parses the fea_app text format (sections ``n``, ``nnz``, ``row_ptr_u32``,
@@ -12,7 +12,7 @@ For each of datasets/pcg_block_jacobi_dataset_{1,2,3}.txt this script
    (max 2000 iterations, rel 1e-4, abs 1e-7) and stores its iteration count,
    residual history and solution in ``case_k/oracle_ref_f32.npz``.
 
-Usage: python tests/golden/make_golden.py [--reference /root/reference]
+Usage: python tests/golden/make_golden.py --reference PATH_TO_REFERENCE_CHECKOUT
 """
 from __future__ import annotations
 
@@ -60,7 +60,7 @@ def parse_text_dataset(path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root of the reference repository checkout")
     args = ap.parse_args()
     oracle.build()
     summary = {}

@@ -102,7 +102,11 @@ def test_product_spmv_bit_exact_csr_and_bsr(ctx):
         m = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], layout=layout)
         dy = torch.full((n,), float("nan"), dtype=torch.float32, device="cuda")
         torch.cuda.synchronize()
-        m.spmv_device(dx.data_ptr(), dy.data_ptr())
+        # Two launches in a row on the matrix's own descriptor, then the
+        # error check that waits for them.
+        for _ in range(2):
+            m.spmv_device(dx.data_ptr(), dy.data_ptr())
+        m.spmv_check()
         ctx.synchronize()
         assert np.array_equal(dy.cpu().numpy().view(np.uint32), ref.view(np.uint32)), layout
 

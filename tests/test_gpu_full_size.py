@@ -1,21 +1,43 @@
-"""Full-size checks through properties that need no oracle run at that size.
+"""Full-size checks: against oracle fixtures, and through properties.
 
+* Oracle parity at 80^3 (fixtures made offline by tests/golden/make_full_size.py
+  from the oracle's runs on the same system): the reference-arithmetic mode
+  gives the FP32 reference oracle's iterations, history and x bit for bit
+  (SHA-256 of all 3,072,000 entries); the product path (CSR and BSR6) gives
+  the FP64-dot oracle's iteration count, its residual history within 1e-4
+  relative, and x within 1e-5 relative on 4096 strided rows, and is within 2 %
+  of the FP32 reference's iterations with x within 1e-5 relative of it.
 * The plain 80^3 lattice (n = 3,072,000, nnz = 127,641,600, BSR6 tiles):
   the solve converges; it is exactly homogeneous (b -> 2b gives the same
   iterations and x -> 2x bit for bit, since scaling by a power of two is
   exact in every FP32 and FP64 operation of the recurrence); the CSR layout
   gives the same iterations and bits; FP64 refinement reaches a true FP64
   relative residual of 1e-8, checked on the host.
-* A batch of 512 systems of lattice side 4..24: every system converges, and
-  a sample solves bit-identically alone.
+* A batch of 512 systems of lattice side 4..24 at relative tolerance 1e-8 with
+  FP64 reductions (the batched configuration): every system converges, a
+  sample solves bit-identically alone, and a sample agrees with the FP64-dot
+  oracle (same iteration count within 1, x within 1e-5 relative).
 """
+import hashlib
+import os
+
 import numpy as np
 import pytest
 
 import oracle
 import wgpu_solver_backend_b200 as wsb
+from conftest import GOLDEN
 
 pytestmark = pytest.mark.gpu
+
+
+def _fixture(name):
+    return np.load(os.path.join(GOLDEN, name))
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
 @pytest.fixture(scope="module")
@@ -23,6 +45,32 @@ def lattice80():
     s = wsb.lattice_generate(80, seed=2024)
     assert s["n"] == 3_072_000 and len(s["values"]) == 127_641_600
     return s
+
+
+def test_80cubed_reference_mode_is_bit_exact_with_the_oracle(ctx, lattice80):
+    s, fx = lattice80, _fixture("lattice80_ref_f32.npz")
+    m = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], layout=wsb.LAYOUT_CSR)
+    x, r = m.solve(s["b"], max_iter=20000, rel_tol=1e-6, precision=wsb.PREC_REFERENCE_F32, history_capacity=20000)
+    assert r["iterations"] == int(fx["iterations"])
+    assert hashlib.sha256(x.tobytes()).hexdigest() == str(fx["x_sha256"])
+    hist = np.asarray(r["history"], np.float32)
+    assert np.array_equal(hist.view(np.uint32), fx["history"].view(np.uint32))
+
+
+@pytest.mark.parametrize("layout", [wsb.LAYOUT_BSR6, wsb.LAYOUT_CSR])
+def test_80cubed_product_path_matches_the_oracles(ctx, lattice80, layout):
+    s, f64, f32 = lattice80, _fixture("lattice80_f64dot.npz"), _fixture("lattice80_ref_f32.npz")
+    m = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], layout=layout)
+    x, r = m.solve(s["b"], max_iter=20000, rel_tol=1e-6, history_capacity=20000)
+    it = int(r["iterations"])
+    # FP64-dot oracle: same arithmetic except the order of the FP64 sums.
+    assert it == int(f64["iterations"])
+    hd = float(np.max(np.abs(r["history"] / f64["history"] - 1.0)))
+    assert hd <= 1e-4, hd
+    assert _rel(x[f64["rows"]], f64["x"]) <= 1e-5, _rel(x[f64["rows"]], f64["x"])
+    # FP32 reference algorithm: iterations within 2 %, solution within 1e-5.
+    assert abs(it - int(f32["iterations"])) <= max(1, 0.02 * int(f32["iterations"]))
+    assert _rel(x[f32["rows"]], f32["x"]) <= 1e-5, _rel(x[f32["rows"]], f32["x"])
 
 
 def test_80cubed_converges_and_is_homogeneous(ctx, lattice80):
@@ -62,12 +110,44 @@ def test_batch_of_512_systems(ctx):
     systems = [wsb.lattice_generate(int(sd), seed=50_000 + i) for i, sd in enumerate(sides)]
     mats = [wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"]) for s in systems]
     bt = wsb.Batch(ctx)
-    ids = [bt.add(m, s["b"], max_iter=20000, rel_tol=1e-6) for m, s in zip(mats, systems)]
+    ids = [bt.add(m, s["b"], max_iter=20000, rel_tol=1e-8) for m, s in zip(mats, systems)]
     bt.solve()
     results = [bt.result(i, s["n"]) for i, s in zip(ids, systems)]
-    assert all(r["rc"] == 0 and r["final_relres"] <= 1e-6 * (1 + 1e-6) for _, r in results)
+    assert all(r["rc"] == 0 and r["final_relres"] <= 1e-8 * (1 + 1e-6) for _, r in results)
     for i in rng.choice(512, 8, replace=False):
-        xa, ra = mats[i].solve(systems[i]["b"], max_iter=20000, rel_tol=1e-6)
+        xa, ra = mats[i].solve(systems[i]["b"], max_iter=20000, rel_tol=1e-8)
         xb, rb = results[i]
         assert rb["iterations"] == ra["iterations"], i
         assert np.array_equal(xb.view(np.uint32), xa.view(np.uint32)), i
+    for i in rng.choice(512, 4, replace=False):
+        s = systems[i]
+        lu = wsb.build_lu_blocks_from_csr_block_starts_6(s["n"], s["row_ptr"], s["col_idx"], s["values"],
+                                                         s["block_starts"])
+        o = oracle.pcg_f64dot(s["row_ptr"], s["col_idx"], s["values"], lu, s["block_starts"], s["b"],
+                              np.zeros(s["n"], np.float32), 20000, 1e-8, 0.0)
+        xb, rb = results[i]
+        assert o["status"] == oracle.OK and abs(int(rb["iterations"]) - int(o["iterations"])) <= 1, i
+        assert _rel(xb, o["x"]) <= 1e-5, (i, _rel(xb, o["x"]))
+
+
+def test_c3_anisotropic_80cubed_refines_to_1e10_against_the_fp64_oracle(ctx):
+    """The mixed-precision configuration at full size: the 80^3 system with
+    every edge stiffness scaled by 10^U(-3,3), FP32 matrix and Krylov vectors,
+    FP64 reductions, FP64 outer refinement (FP64 true residual, inner FP32 PCG
+    to 1e-4 per sweep) to a true FP64 relative residual of 1e-10, recomputed
+    on the host. The error is stated against the full FP64 PCG oracle's
+    solution (relative residual 4.9e-12; fixture aniso80_f64.npz) on 4096
+    strided rows."""
+    s = wsb.lattice_generate(80, seed=2024, aniso_log10=3.0)
+    fx = _fixture("aniso80_f64.npz")
+    m = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"])
+    x64 = np.zeros(s["n"], np.float64)
+    x, r = m.solve(s["b"], max_iter=400000, rel_tol=0.0, precision=wsb.PREC_MIXED_F64_IR, target_relres=1e-10,
+                   inner_rel_tol=1e-4, max_refine=50, x64_out=x64)
+    assert r["rc"] == 0, r
+    tr = oracle.true_relres_f64(s["row_ptr"], s["col_idx"], s["values"], s["b"], x64)
+    err = _rel(x64[fx["rows"]], fx["x"])
+    print(f"C3: sweeps={r['refine_sweeps']} iterations={r['iterations']} true_relres={tr:.3e} "
+          f"err_vs_fp64_oracle={err:.3e}")
+    assert tr <= 1e-10, tr
+    assert err <= 1e-6, err

@@ -120,6 +120,12 @@ class GpuContext:
     def set_stream(self, cuda_stream_ptr: int | None):
         _check(_lib_handle().wsb_context_set_stream(self.handle, C.c_void_p(cuda_stream_ptr or 0)), self.handle)
 
+    def set_wait_limit(self, cycles: int = 0):
+        """Limit of every pipeline wait in the solver kernels, in SM clock
+        cycles (0: the default of about 2 s). A wait that runs out ends the
+        solves in flight with status TIMEOUT."""
+        _check(_lib_handle().wsb_context_set_wait_limit(self.handle, int(cycles)), self.handle)
+
     def synchronize(self):
         _check(_lib_handle().wsb_context_synchronize(self.handle), self.handle)
 
@@ -430,8 +436,13 @@ class Matrix:
         return dict(spmv_ms=ms[0], update_ms=ms[1], pupdate_ms=ms[2])
 
     def spmv_device(self, d_x: int, d_y: int):
+        """y = A x on the context's stream (not waited for)."""
         _check(_lib_handle().wsb_matrix_spmv_device(self.ctx.handle, self.handle, C.c_void_p(d_x), C.c_void_p(d_y)),
                self.ctx.handle)
+
+    def spmv_check(self):
+        """Waits for the last spmv_device launch; raises on a kernel error."""
+        _check(_lib_handle().wsb_matrix_spmv_check(self.ctx.handle, self.handle), self.ctx.handle)
 
     def __del__(self):
         if getattr(self, "handle", None):
@@ -481,17 +492,24 @@ class Batch:
 class Server:
     """Continuous-batching solve server (wsb_server_*)."""
 
-    def __init__(self, ctx: GpuContext, memory_budget_bytes=0, max_active=0, iters_per_step=0):
+    def __init__(self, ctx: GpuContext, memory_budget_bytes=0, max_active=0, iters_per_step=0, borrow_inputs=False,
+                 device_prep=False):
+        """borrow_inputs: requests read the submitted arrays in place (this
+        object keeps them alive until the request is done) instead of copying
+        them at submit. device_prep: each request's column check, BSR6
+        conversion and LU run on the GPU instead of the host."""
         self.ctx = ctx
         so = ServerOpts()
         so.struct_size = C.sizeof(ServerOpts)
         so.memory_budget_bytes = int(memory_budget_bytes)
         so.max_active = int(max_active)
         so.iters_per_step = int(iters_per_step)
+        so.flags = (_lib.SERVER_BORROW_INPUTS if borrow_inputs else 0) | (_lib.SERVER_DEVICE_PREP if device_prep else 0)
         h = C.c_void_p()
         _check(_lib_handle().wsb_server_create(ctx.handle, C.byref(so), C.byref(h)), ctx.handle)
         self.handle = h
         self._n = {}
+        self._borrowed = {}  # request id -> arrays the server reads in place
 
     def submit(self, row_ptr, col_idx, values, block_starts, b, x0=None, max_iter=2000, rel_tol=1e-8, abs_tol=0.0,
                precision=PREC_F32_F64DOT, **mixed) -> int:
@@ -505,6 +523,7 @@ class Server:
                                                _p(x0, _lib.f32p), int(max_iter), float(rel_tol), float(abs_tol),
                                                C.byref(o), C.byref(rid)), self.ctx.handle)
         self._n[rid.value] = n
+        self._borrowed[rid.value] = (rp, ci, v, bs, b, x0)
         return rid.value
 
     def poll(self, rid: int):
@@ -514,6 +533,7 @@ class Server:
         if rc == _lib.PENDING:
             return None
         self._n.pop(rid, None)
+        self._borrowed.pop(rid, None)
         out = _result_dict(res)
         out["rc"] = rc
         return x, out
@@ -525,6 +545,7 @@ class Server:
         if rc == _lib.TIMEOUT:
             raise WsbError(rc, _lib_handle().wsb_last_error(self.ctx.handle).decode())
         self._n.pop(rid, None)
+        self._borrowed.pop(rid, None)
         out = _result_dict(res)
         out["rc"] = rc
         return x, out
@@ -538,6 +559,7 @@ class Server:
         if getattr(self, "handle", None):
             _lib_handle().wsb_server_destroy(self.handle)
             self.handle = None
+        self._borrowed = {}
 
     def __del__(self):
         self.close()

@@ -54,16 +54,20 @@ class TuneResult(C.Structure):
                 ("reserved", C.c_uint32)]
 
 
+SERVER_BORROW_INPUTS, SERVER_DEVICE_PREP = 1, 2
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("max_active", C.c_uint32), ("memory_budget_bytes", C.c_uint64),
-                ("iters_per_step", C.c_uint32), ("reserved", C.c_uint32)]
+                ("iters_per_step", C.c_uint32), ("flags", C.c_uint32)]
 
 
 class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
                 ("rejected", C.c_uint64), ("active", C.c_uint64), ("pending", C.c_uint64), ("steps", C.c_uint64),
                 ("device_bytes_in_use", C.c_uint64), ("device_bytes_peak", C.c_uint64), ("busy_ms", C.c_double),
-                ("kernel_launches", C.c_uint64)]
+                ("kernel_launches", C.c_uint64), ("host_prep_ms", C.c_double), ("upload_ms", C.c_double),
+                ("admit_ms", C.c_double), ("retire_ms", C.c_double), ("sched_idle_ms", C.c_double)]
 
 
 class LatticeSizes(C.Structure):
@@ -120,6 +124,8 @@ SIGNATURES = {
     "wsb_solve_device": (C.c_int, [vp, vp, vp, vp, C.c_uint64, C.c_float, C.c_float, C.POINTER(SolveOpts),
                                    C.POINTER(SolveResult)]),
     "wsb_matrix_spmv_device": (C.c_int, [vp, vp, vp, vp]),
+    "wsb_matrix_spmv_check": (C.c_int, [vp, vp]),
+    "wsb_context_set_wait_limit": (C.c_int, [vp, C.c_uint64]),
     "wsb_matrix_kernel_times": (C.c_int, [vp, vp, vp, C.c_uint32, f64p]),
     "wsb_batch_create": (C.c_int, [vp, C.POINTER(vp)]),
     "wsb_batch_add": (C.c_int, [vp, vp, f32p, f32p, C.c_uint64, C.c_float, C.c_float, C.POINTER(SolveOpts),

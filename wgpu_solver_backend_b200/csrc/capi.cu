@@ -229,6 +229,21 @@ struct wsb_matrix {
     std::unique_ptr<Engine> eng;
     uint32_t slot = 0;
     SolveCfg slot_cfg;
+    // wsb_matrix_spmv_device: the plain SpMV kernel's one-system descriptor
+    // and error word (device), allocated on the first call and owned by the
+    // matrix; a pinned host copy of the error word refreshed after every
+    // launch, and the event that marks that copy.
+    SysDesc *spmv_dd = nullptr;
+    StepParams *spmv_sp = nullptr;
+    uint32_t *spmv_err_h = nullptr;
+    cudaEvent_t spmv_err_ev = nullptr;
+    bool spmv_err_pending = false;
+    ~wsb_matrix() {
+        dev_free(spmv_dd);
+        dev_free(spmv_sp);
+        if (spmv_err_h) cudaFreeHost(spmv_err_h);
+        if (spmv_err_ev) cudaEventDestroy(spmv_err_ev);
+    }
 };
 
 #define CHECK_CTX(c)                                                              \
@@ -313,6 +328,12 @@ extern "C" int wsb_context_adapter_info(const wsb_context *ctx, wsb_adapter_info
 extern "C" int wsb_context_set_stream(wsb_context *ctx, void *stream) {
     CHECK_CTX(ctx);
     ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return WSB_OK;
+}
+
+extern "C" int wsb_context_set_wait_limit(wsb_context *ctx, uint64_t cycles) {
+    CHECK_CTX(ctx);
+    ctx->wait_cycles = cycles;
     return WSB_OK;
 }
 
@@ -801,10 +822,43 @@ extern "C" int wsb_solve_device(wsb_context *ctx, wsb_matrix *m, const float *d_
     return matrix_solve(ctx, m, d_b, d_x, true, max_iter, rel, abs_tol, o, res);
 }
 
+// The error word of the plain SpMV kernel is sticky: launches OR their codes
+// into it and only a reported error clears it, so a code survives later
+// launches until a call reads it.
+static int spmv_error_status(wsb_matrix *m, uint32_t code) {
+    m->spmv_err_pending = false;
+    *m->spmv_err_h = 0;
+    cudaMemsetAsync(&m->spmv_sp->error, 0, sizeof(uint32_t), m->ctx->stream);
+    return fail(m->ctx, (code & kErrWaitMask) ? WSB_ERR_TIMEOUT : WSB_ERR_CUDA,
+                "an earlier wsb_matrix_spmv_device launch on this matrix failed (kernel code %u)", code);
+}
+
 extern "C" int wsb_matrix_spmv_device(wsb_context *ctx, wsb_matrix *m, const float *d_x, float *d_y) {
     CHECK_CTX(ctx);
     if (!m || !d_x || !d_y) return fail(ctx, WSB_ERR_BAD_INPUT, "bad arguments");
-    // A one-system descriptor for the plain SpMV kernel.
+    if (m->ctx->device != ctx->device)
+        return fail(ctx, WSB_ERR_BAD_INPUT, "the matrix lives on device %d, the context on device %d", m->ctx->device,
+                    ctx->device);
+    if (!m->spmv_dd) {
+        void *dd = nullptr, *sp = nullptr;
+        WSB_CUDA_TRY(ctx, cudaMalloc(&dd, sizeof(SysDesc)));
+        m->spmv_dd = static_cast<SysDesc *>(dd);
+        WSB_CUDA_TRY(ctx, cudaMalloc(&sp, sizeof(StepParams)));
+        m->spmv_sp = static_cast<StepParams *>(sp);
+        WSB_CUDA_TRY(ctx, cudaMemsetAsync(m->spmv_sp, 0, sizeof(StepParams), ctx->stream));
+        WSB_CUDA_TRY(ctx, cudaHostAlloc((void **)&m->spmv_err_h, sizeof(uint32_t), cudaHostAllocDefault));
+        *m->spmv_err_h = 0;
+        WSB_CUDA_TRY(ctx, cudaEventCreateWithFlags(&m->spmv_err_ev, cudaEventDisableTiming));
+        WSB_CUDA_TRY(ctx, cudaFuncSetAttribute(k_spmv_plain, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)kSpmvSmem));
+    }
+    // A finished read-back of the error word with a code in it: report it.
+    if (m->spmv_err_pending && cudaEventQuery(m->spmv_err_ev) == cudaSuccess) {
+        m->spmv_err_pending = false;
+        if (*m->spmv_err_h) return spmv_error_status(m, *m->spmv_err_h);
+    }
+    // The one-system descriptor (rewritten every call: the tiles may have
+    // been rebuilt by the autotuner since the last one).
     SysDesc d;
     std::memset(&d, 0, sizeof d);
     d.n = m->A.n;
@@ -817,26 +871,26 @@ extern "C" int wsb_matrix_spmv_device(wsb_context *ctx, wsb_matrix *m, const flo
     d.bval = m->A.bval;
     d.stiles = m->A.stiles;
     d.n_stiles = m->A.n_stiles;
-    // Per-thread, per-device scratch for the descriptor and the error word.
-    struct Scratch {
-        SysDesc *dd = nullptr;
-        StepParams *sp = nullptr;
-        int dev = -1;
-    };
-    static thread_local Scratch sc;
-    if (!sc.dd || sc.dev != ctx->device) {
-        WSB_CUDA_TRY(ctx, cudaMalloc(&sc.dd, sizeof(SysDesc)));
-        WSB_CUDA_TRY(ctx, cudaMalloc(&sc.sp, sizeof(StepParams)));
-        WSB_CUDA_TRY(ctx, cudaMemsetAsync(sc.sp, 0, sizeof(StepParams), ctx->stream));
-        sc.dev = ctx->device;
-        cudaFuncSetAttribute(k_spmv_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpmvSmem);
-    }
-    WSB_CUDA_TRY(ctx, cudaMemcpyAsync(sc.dd, &d, sizeof d, cudaMemcpyHostToDevice, ctx->stream));
+    WSB_CUDA_TRY(ctx, cudaMemcpyAsync(m->spmv_dd, &d, sizeof d, cudaMemcpyHostToDevice, ctx->stream));
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_spmv_plain, kSpmvThreads, kSpmvSmem);
     const uint32_t g = std::max<uint32_t>(1, std::min<uint32_t>(m->A.n_stiles, (uint32_t)(std::max(occ, 1) * ctx->sm_count)));
-    k_spmv_plain<<<g, kSpmvThreads, kSpmvSmem, ctx->stream>>>(sc.dd, sc.sp, d_x, d_y);
+    k_spmv_plain<<<g, kSpmvThreads, kSpmvSmem, ctx->stream>>>(m->spmv_dd, m->spmv_sp, d_x, d_y);
     WSB_CUDA_TRY(ctx, cudaGetLastError());
+    WSB_CUDA_TRY(ctx, cudaMemcpyAsync(m->spmv_err_h, &m->spmv_sp->error, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+    WSB_CUDA_TRY(ctx, cudaEventRecord(m->spmv_err_ev, ctx->stream));
+    m->spmv_err_pending = true;
+    return WSB_OK;
+}
+
+extern "C" int wsb_matrix_spmv_check(wsb_context *ctx, wsb_matrix *m) {
+    CHECK_CTX(ctx);
+    if (!m) return fail(ctx, WSB_ERR_BAD_INPUT, "matrix is null");
+    if (!m->spmv_err_pending) return WSB_OK;
+    WSB_CUDA_TRY(ctx, cudaEventSynchronize(m->spmv_err_ev));
+    m->spmv_err_pending = false;
+    if (*m->spmv_err_h) return spmv_error_status(m, *m->spmv_err_h);
     return WSB_OK;
 }
 

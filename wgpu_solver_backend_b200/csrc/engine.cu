@@ -639,6 +639,7 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
     h_sp_->n_work_b = n_work_b_;
     h_sp_->n_work_c = n_work_c_;
     h_sp_->error = 0;
+    h_sp_->wait_cycles = ctx_->wait_cycles;
     // Bound the device loop by the largest remaining iteration budget: every
     // system stops by its own max_iter, so the loop ends even if one did not.
     uint64_t budget = 1;
@@ -775,6 +776,7 @@ int Engine::profile_kernels(uint32_t s, uint32_t iters, double ms[5]) {
     h_sp_->n_work_b = n_work_b_;
     h_sp_->n_work_c = n_work_c_;
     h_sp_->error = 0;
+    h_sp_->wait_cycles = ctx_->wait_cycles;
     h_sp_->num_active = 1;
     h_sp_->loop_count = 0;
     h_sp_->loop_limit = iters;

@@ -114,19 +114,28 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 
 constexpr long long kWaitCycles = 4000000000ll;  // about 2 s at 1.9 GHz
 
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+// The limit of the pipeline waits of one launch: StepParams::wait_cycles, or
+// kWaitCycles when that is 0. The drains of a CTA's own copies in flight
+// always use kWaitCycles (a CTA must not leave while a copy into its shared
+// memory may still land).
+__device__ __forceinline__ long long wait_limit(const StepParams *sp) {
+    const unsigned long long w = sp->wait_cycles;
+    return w == 0 ? kWaitCycles : (long long)(w > (unsigned long long)kWaitCycles ? kWaitCycles : w);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long lim = kWaitCycles) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > kWaitCycles) return false;
+        if (clock64() - t0 > lim) return false;
     return true;
 }
 
 // A phase that another thread of the CTA has already seen complete: a
 // non-blocking check (which also makes the phase's data visible to this
 // thread), with the bounded wait as a fallback.
-__device__ __forceinline__ void mbar_observe(uint64_t *bar, uint32_t parity) {
-    if (!mbar_test_wait(bar, parity)) mbar_wait(bar, parity);
+__device__ __forceinline__ void mbar_observe(uint64_t *bar, uint32_t parity, long long lim) {
+    if (!mbar_test_wait(bar, parity)) mbar_wait(bar, parity, lim);
 }
 
 // Programmatic dependent launch: the next kernel in the stream may start
@@ -275,7 +284,8 @@ __device__ __forceinline__ bool take_ticket(uint32_t *counter, uint32_t cnt, uin
 enum SpmvMode { M_LOOP = 0, M_INIT = 1, M_PLAIN = 2 };
 
 // Stage layout (floats), from kernels_fused.cuh: CSR values [0, kCsrCap+8),
-// columns at kColOff; BSR6 block values [0, 36 kBsrCapBlocks), block columns
+// the gathered x[col] of every staged value at kColOff (same index as the
+// value); BSR6 block values [0, 36 kBsrCapBlocks), block columns
 // at kBcolOff, gathered x at kXgOff (float2, 3 per block); row pointers at
 // kRpOff.
 constexpr int NC = kSpmvConsumers;  // consumer threads of the SpMV kernels
@@ -301,7 +311,7 @@ struct SpmvDesc {
     const uint32_t *rptr;  // the tile's row pointers: row_ptr + r0 or brow_ptr + r0
     const uint32_t *cols;  // BSR6: the tile's block columns, bcol + k0
     const float *vsrc;     // bulk-copy source of the values: bval + 36 k0, or val + ka
-    const uint32_t *csrc;  // CSR: bulk-copy source of the columns, col + ka
+    const uint32_t *csrc;  // CSR: the staged range's columns, col + ka (read by the gather warp)
 };
 
 template <int kMode>
@@ -370,23 +380,56 @@ __device__ __forceinline__ void issue_spmv(const SpmvDesc &d, float *stage, uint
         if (vb) tma_load_stream(stage, d.vsrc, vb, bar, pol);
     } else {
         const uint32_t cc = ((d.k1 - d.ka) + 3) & ~3u;
-        mbar_expect_tx(bar, 8u * cc);
-        if (cc) {
-            tma_load_stream(stage, d.vsrc, 4u * cc, bar, pol);
-            tma_load_stream(stage + kColOff, d.csrc, 4u * cc, bar, pol);
+        mbar_expect_tx(bar, 4u * cc);
+        if (cc) tma_load_stream(stage, d.vsrc, 4u * cc, bar, pol);
+    }
+}
+
+// Gather warp, CSR tile: x[col[j]] for every staged index j of [ka, ka + cc)
+// into xg[j - ka] by 4-byte cp.async. The columns are read here with
+// streaming 16-byte loads (8 in flight per lane) and never staged; indices
+// outside [k0, k1) belong to neighbouring tiles or the zero padding of the
+// column array, so every gathered address is a valid row of x.
+__device__ __forceinline__ void gather_csr(const SpmvDesc &d, float *stage, uint32_t lane) {
+    const float *__restrict__ xin = d.x;
+    float *xg = stage + kColOff;
+    const uint4 *__restrict__ c4 = reinterpret_cast<const uint4 *>(d.csrc);
+    const uint32_t nq = (((d.k1 - d.ka) + 3) & ~3u) >> 2;  // 16-byte groups of columns
+    constexpr uint32_t kBatch = 8;
+    for (uint32_t q0 = 0; q0 < nq; q0 += 32u * kBatch) {
+        uint4 c[kBatch];
+#pragma unroll
+        for (uint32_t u = 0; u < kBatch; ++u) {
+            const uint32_t q = q0 + lane + 32u * u;
+            c[u] = q < nq ? __ldcs(c4 + q) : make_uint4(0u, 0u, 0u, 0u);
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < kBatch; ++u) {
+            const uint32_t q = q0 + lane + 32u * u;
+            if (q < nq) {
+                float *dst = xg + 4u * q;
+                cp_async4(dst + 0, xin + c[u].x);
+                cp_async4(dst + 1, xin + c[u].y);
+                cp_async4(dst + 2, xin + c[u].z);
+                cp_async4(dst + 3, xin + c[u].w);
+            }
         }
     }
 }
 
 // Gather warp, one tile (32 lanes): the tile's row pointers into the stage
-// (rp[i] = row_ptr[r0 + i], i <= nr), and for BSR6 its block columns (bcol[i]
-// = block column of block k0 + i) and the 6 x values of every block column,
-// as 3 float2 per block, by cp.async. None of this waits for the tile's bulk
-// copy, so the gathers run while the block values stream in.
+// (rp[i] = row_ptr[r0 + i], i <= nr); for CSR the x value of every staged
+// nonzero (gather_csr); for BSR6 its block columns (bcol[i] = block column of
+// block k0 + i) and the 6 x values of every block column, as 3 float2 per
+// block, by cp.async. None of this waits for the tile's bulk copy, so the
+// gathers run while the values stream in.
 __device__ __forceinline__ void gather_tile(const SpmvDesc &d, float *stage, uint32_t lane) {
     uint32_t *rp = reinterpret_cast<uint32_t *>(stage + kRpOff);
     for (uint32_t i = lane; i <= d.nr; i += 32u) rp[i] = __ldg(d.rptr + i);
-    if (d.layout != LAYOUT_BSR6) return;
+    if (d.layout != LAYOUT_BSR6) {
+        gather_csr(d, stage, lane);
+        return;
+    }
     const float *__restrict__ xin = d.x;
     const bool al8 = (reinterpret_cast<uintptr_t>(xin) & 7u) == 0;
     uint32_t *bcol = reinterpret_cast<uint32_t *>(stage + kBcolOff);
@@ -420,29 +463,28 @@ __device__ __forceinline__ void gather_tile(const SpmvDesc &d, float *stage, uin
     }
 }
 
-// CSR tile from a filled stage: products val*x[col] in place (all consumer
-// threads, strided over the nonzeros), then one thread per row adds its
-// products in index order (spmv.wgsl:58-61).
-__device__ __forceinline__ float csr_stage(const SpmvDesc &d, const float *__restrict__ xin, float *stage) {
-    float *val = stage;
-    const uint32_t *col = reinterpret_cast<const uint32_t *>(stage + kColOff);
+// CSR tile from a filled and gathered stage: one thread per row adds
+// val[j] * x[col[j]] over its nonzeros in index order, each product rounded
+// before the add (spmv.wgsl:58-61); both factors come from the stage.
+__device__ __forceinline__ float csr_stage(const SpmvDesc &d, const float *stage) {
+    const float *val = stage;
+    const float *xg = stage + kColOff;
     const uint32_t *rp = reinterpret_cast<const uint32_t *>(stage + kRpOff);
-    const uint32_t j0 = d.k0 - d.ka, j1 = d.k1 - d.ka;
-    uint32_t j = j0 + threadIdx.x;
-    for (; j + 7 * NC < j1; j += 8 * NC) {
-        float xv[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) xv[q] = __ldg(xin + col[j + q * NC]);
-#pragma unroll
-        for (int q = 0; q < 8; ++q) val[j + q * NC] = __fmul_rn(val[j + q * NC], xv[q]);
-    }
-    for (; j < j1; j += NC) val[j] = __fmul_rn(val[j], __ldg(xin + col[j]));
-    csync<NC>();
     float acc = 0.0f;
     if (threadIdx.x < d.nr) {
         const uint32_t o = threadIdx.x;
         const uint32_t s = rp[o] - d.ka, e = rp[o + 1] - d.ka;
-        for (uint32_t q = s; q < e; ++q) acc = __fadd_rn(acc, val[q]);
+        uint32_t q = s;
+        // Operands two products ahead, so shared-memory latency overlaps the add chain.
+        for (; q + 4u <= e; q += 4u) {
+            const float v0 = val[q], v1 = val[q + 1], v2 = val[q + 2], v3 = val[q + 3];
+            const float x0 = xg[q], x1 = xg[q + 1], x2 = xg[q + 2], x3 = xg[q + 3];
+            acc = __fadd_rn(acc, __fmul_rn(v0, x0));
+            acc = __fadd_rn(acc, __fmul_rn(v1, x1));
+            acc = __fadd_rn(acc, __fmul_rn(v2, x2));
+            acc = __fadd_rn(acc, __fmul_rn(v3, x3));
+        }
+        for (; q < e; ++q) acc = __fadd_rn(acc, __fmul_rn(val[q], xg[q]));
     }
     return acc;
 }
@@ -584,7 +626,8 @@ __device__ __forceinline__ void flush_spmv(const SysDesc *__restrict__ sys, uint
 template <int kMode>
 __device__ __forceinline__ void spmv_producer(const SysDesc *__restrict__ sys, StepParams *sp,
                                               const float *xplain, float *yplain, float *smem, uint64_t *full,
-                                              uint64_t *meta, uint64_t *empty, SpmvDesc *desc, SpmvDesc *bdesc) {
+                                              uint64_t *meta, uint64_t *empty, SpmvDesc *desc, SpmvDesc *bdesc,
+                                              long long lim) {
     constexpr uint32_t NS = kSpmvStages;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t G = gridDim.x;
@@ -610,7 +653,7 @@ __device__ __forceinline__ void spmv_producer(const SysDesc *__restrict__ sys, S
             const uint32_t n_out = more ? cnt : cnt + kGatherWarps;
             for (uint32_t i = 0; i < n_out; ++i) {
                 const uint32_t s = k % NS;
-                if (k >= NS && !mbar_wait(&empty[s], ((k / NS) - 1) & 1u)) {
+                if (k >= NS && !mbar_wait(&empty[s], ((k / NS) - 1) & 1u, lim)) {
                     atomicOr(&sp->error, kErrSpmvProducerWait);
                     err = true;
                     break;
@@ -647,19 +690,19 @@ __device__ __forceinline__ void spmv_producer(const SysDesc *__restrict__ sys, S
 template <int kMode>
 __device__ __forceinline__ void spmv_gatherer(const SysDesc *__restrict__ sys, StepParams *sp,
                                               const float *__restrict__ xplain, float *smem, uint64_t *meta,
-                                              uint64_t *gath, const SpmvDesc *desc, uint32_t g) {
+                                              uint64_t *gath, const SpmvDesc *desc, uint32_t g, long long lim) {
     constexpr uint32_t NS = kSpmvStages;
     const uint32_t lane = threadIdx.x & 31u;
     for (uint32_t j = g;; j += kGatherWarps) {
         const uint32_t s = j % NS, par = (j / NS) & 1u;
         uint32_t ok = 1;
-        if (lane == 0) ok = mbar_wait(&meta[s], par) ? 1u : 0u;
+        if (lane == 0) ok = mbar_wait(&meta[s], par, lim) ? 1u : 0u;
         ok = __shfl_sync(0xffffffffu, ok, 0);
         if (!ok) {
             if (lane == 0) atomicOr(&sp->error, kErrGatherWait);
             break;
         }
-        mbar_wait(&meta[s], par);  // completed: the descriptor is visible
+        mbar_observe(&meta[s], par, lim);  // completed: the descriptor is visible
         const SpmvDesc d = desc[s];
         if (d.valid && !d.lng) gather_tile(d, smem + s * kSpmvStageFloats, lane);
         mbar_arrive(&gath[s]);
@@ -697,9 +740,10 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
     }
     __syncthreads();
     pdl_start();
+    const long long lim = wait_limit(sp);
     if (tid >= NC) {
-        if (tid < NC + 32) spmv_producer<kMode>(sys, sp, xplain, yplain, smem, full, meta, empty, desc, bdesc);
-        else spmv_gatherer<kMode>(sys, sp, xplain, smem, meta, gath, desc, (tid - NC - 32) >> 5);
+        if (tid < NC + 32) spmv_producer<kMode>(sys, sp, xplain, yplain, smem, full, meta, empty, desc, bdesc, lim);
+        else spmv_gatherer<kMode>(sys, sp, xplain, smem, meta, gath, desc, (tid - NC - 32) >> 5, lim);
         return;
     }
     uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles of run_sys published since the last ticket
@@ -708,14 +752,14 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
         const uint32_t s = k % NS, par = (k / NS) & 1u;
         // Thread 0 waits (bounded) and shares the outcome through a flag that
         // alternates with k, so a later write never meets an earlier read.
-        if (tid == 0) s_ok[k & 1u] = (mbar_wait(&gath[s], par) && mbar_wait(&full[s], par)) ? 1 : 0;
+        if (tid == 0) s_ok[k & 1u] = (mbar_wait(&gath[s], par, lim) && mbar_wait(&full[s], par, lim)) ? 1 : 0;
         csync<NC>();
         if (!s_ok[k & 1u]) {
             if (tid == 0) atomicOr(&sp->error, kErrSpmvConsumerWait);
             return;
         }
-        mbar_observe(&gath[s], par);
-        mbar_observe(&full[s], par);
+        mbar_observe(&gath[s], par, lim);
+        mbar_observe(&full[s], par, lim);
         // The descriptor is read in place: it stays valid until this stage
         // is handed back; what is needed after that is copied first.
         const SpmvDesc &d = desc[s];
@@ -737,20 +781,24 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
         }
         const uint32_t row0 = d.layout == LAYOUT_BSR6 ? 6u * d.r0 : d.r0;
         const uint32_t nrows = d.layout == LAYOUT_BSR6 ? 6u * d.nr : d.nr;
-        const bool gathered = !d.lng && d.layout == LAYOUT_BSR6;
+        const bool bsr_gathered = !d.lng && d.layout == LAYOUT_BSR6;
         float acc, p_own = 0.0f;
         bool own_ok = false;
-        if (gathered) {
+        if (bsr_gathered) {
             acc = bsr_stage<kMode == M_LOOP>(d, stage, &p_own, &own_ok);
         } else {
             if (kMode == M_LOOP && tid < nrows) {
                 p_own = __ldg(d.x + row0 + tid);
                 own_ok = true;
             }
-            acc = d.lng ? long_tile(sys[d.sys], d, d.x, stage) : csr_stage(d, d.x, stage);
-            // These paths wrote into the stage: order those writes before the
-            // bulk copy that will next fill it.
-            fence_proxy_async();
+            if (d.lng) {
+                acc = long_tile(sys[d.sys], d, d.x, stage);
+                // That path wrote into the stage: order those writes before
+                // the bulk copy that will next fill it.
+                fence_proxy_async();
+            } else {
+                acc = csr_stage(d, stage);
+            }
         }
         float *const yv = d.y;
         const float *const xv = d.x;
@@ -1055,7 +1103,8 @@ __device__ __forceinline__ void flush_upd(const SysDesc *__restrict__ sys, StepP
 // discipline as the SpMV producer.
 template <bool kInit>
 __device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, StepParams *sp, float *smem,
-                                             uint64_t *full, uint64_t *empty, UpdDesc *desc, UpdDesc *bdesc) {
+                                             uint64_t *full, uint64_t *empty, UpdDesc *desc, UpdDesc *bdesc,
+                                             long long lim) {
     constexpr uint32_t NS = kUpdStages;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t G = gridDim.x;
@@ -1081,7 +1130,7 @@ __device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, St
             const uint32_t n_out = more ? cnt : cnt + kUpdGroups;
             for (uint32_t i = 0; i < n_out; ++i) {
                 const uint32_t s = k % NS;
-                if (k >= NS && !mbar_wait(&empty[s], ((k / NS) - 1) & 1u)) {
+                if (k >= NS && !mbar_wait(&empty[s], ((k / NS) - 1) & 1u, lim)) {
                     atomicOr(&sp->error, kErrUpdProducerWait);
                     err = true;
                     break;
@@ -1129,7 +1178,7 @@ struct UpdGroupSmem {
 template <bool kInit, int G>
 __device__ __forceinline__ void upd_consumers(const SysDesc *__restrict__ sys, StepParams *sp, float *smem,
                                               uint64_t *full, uint64_t *empty, const UpdDesc *desc,
-                                              UpdGroupSmem &g) {
+                                              UpdGroupSmem &g, long long lim) {
     constexpr uint32_t NS = kUpdStages;
     constexpr int GT = NU / kUpdGroups;  // threads of the group
     constexpr int BAR = 1 + G;           // its named barrier
@@ -1141,13 +1190,13 @@ __device__ __forceinline__ void upd_consumers(const SysDesc *__restrict__ sys, S
     uint32_t n = 0;  // tiles this group has taken
     for (uint32_t k = G;; k += kUpdGroups, ++n) {
         const uint32_t s = k % NS, par = (k / NS) & 1u;
-        if (lt == 0) g.s_ok[n & 1u] = mbar_wait(&full[s], par) ? 1 : 0;
+        if (lt == 0) g.s_ok[n & 1u] = mbar_wait(&full[s], par, lim) ? 1 : 0;
         gsync<GT, BAR>();
         if (!g.s_ok[n & 1u]) {
             if (lt == 0) atomicOr(&sp->error, kInit ? kErrInitConsumerWait : kErrUpdConsumerWait);
             return;
         }
-        mbar_observe(&full[s], par);
+        mbar_observe(&full[s], par, lim);
         // The descriptor is read in place: it stays valid until this stage
         // is handed back; what is needed after that is copied first.
         const UpdDesc &d = desc[s];
@@ -1246,14 +1295,15 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
         gsm[i / kUpdTileRows].sflag[i % kUpdTileRows] = 0u;
     __syncthreads();
     pdl_start();
+    const long long lim = wait_limit(sp);
     if (tid >= NU) {
-        if (tid < NU + 32) upd_producer<kInit>(sys, sp, smem, full, empty, desc, bdesc);
+        if (tid < NU + 32) upd_producer<kInit>(sys, sp, smem, full, empty, desc, bdesc, lim);
         return;
     }
     const uint32_t grp = tid / (NU / kUpdGroups);
-    if (grp == 0) upd_consumers<kInit, 0>(sys, sp, smem, full, empty, desc, gsm[0]);
+    if (grp == 0) upd_consumers<kInit, 0>(sys, sp, smem, full, empty, desc, gsm[0], lim);
     if constexpr (kUpdGroups > 1) {
-        if (grp == 1) upd_consumers<kInit, 1>(sys, sp, smem, full, empty, desc, gsm[1]);
+        if (grp == 1) upd_consumers<kInit, 1>(sys, sp, smem, full, empty, desc, gsm[1], lim);
     }
 }
 
@@ -1362,7 +1412,51 @@ __global__ void k_loop_gate(StepParams *sp, cudaGraphConditionalHandle h) {
 // Mixed precision (FP64 outer iterative refinement).
 // k_resid64: r64 = b - A x64 with FP32 matrix entries and FP64 accumulation;
 // the inner right-hand side becomes (float) r64; FP64 ||r64||^2 and ||b||^2.
+// One work item is one update tile (<= 256 rows). BSR6: one thread per row,
+// which walks its block row four blocks at a time with every load of the four
+// issued before the first multiply (block columns, then 3 float2 of the row's
+// block values and 3 double2 of x64 per block). CSR: eight lanes per row,
+// striding over the row's nonzeros (32-byte coalesced runs of values and
+// columns), then a fixed shuffle tree. FP64 sums need no particular order
+// here (the result only has to be an accurate FP64 residual), but the order
+// is fixed, so a system's residual does not depend on what else runs.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ double resid_row_bsr6(const SysDesc &S, uint32_t i) {
+    const uint32_t br = i / 6u, a = i - 6u * br;
+    const uint32_t k0 = __ldg(S.brow_ptr + br), k1 = __ldg(S.brow_ptr + br + 1);
+    const double2 *__restrict__ x2 = reinterpret_cast<const double2 *>(S.x64);
+    double s = 0.0;
+    for (uint32_t k = k0; k < k1; k += 4u) {
+        uint32_t c[4];
+        float2 v[4][3];
+#pragma unroll
+        for (uint32_t u = 0; u < 4; ++u) c[u] = k + u < k1 ? __ldg(S.bcol + k + u) : 0u;
+#pragma unroll
+        for (uint32_t u = 0; u < 4; ++u) {
+            if (k + u < k1) {
+                const float2 *B = reinterpret_cast<const float2 *>(S.bval + (size_t)(k + u) * 36u + a * 6u);
+                v[u][0] = __ldcs(B);
+                v[u][1] = __ldcs(B + 1);
+                v[u][2] = __ldcs(B + 2);
+            }
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < 4; ++u) {
+            if (k + u < k1) {
+                const double2 *X = x2 + 3u * (size_t)c[u];
+                const double2 y0 = X[0], y1 = X[1], y2 = X[2];
+                s += (double)v[u][0].x * y0.x;
+                s += (double)v[u][0].y * y0.y;
+                s += (double)v[u][1].x * y1.x;
+                s += (double)v[u][1].y * y1.y;
+                s += (double)v[u][2].x * y2.x;
+                s += (double)v[u][2].y * y2.y;
+            }
+        }
+    }
+    return s;
+}
+
 __global__ void __launch_bounds__(kThreads) k_resid64(const SysDesc *__restrict__ sys, StepParams *sp) {
     __shared__ double red[64];
     __shared__ int s_last;
@@ -1379,27 +1473,48 @@ __global__ void __launch_bounds__(kThreads) k_resid64(const SysDesc *__restrict_
         SysState *st = S.st;
         const UpdTile T = S.utiles[it.tile];
         const uint32_t rows = T.row1 - T.row0;
+        float *const bin = const_cast<float *>(S.b);
         double rr = 0.0, bb = 0.0;
-        if (t < rows) {
-            const uint32_t i = T.row0 + t;
-            const double *__restrict__ x64 = S.x64;
-            double s = 0.0;
-            if (S.layout == LAYOUT_BSR6) {
-                const uint32_t br = i / 6u, a = i - 6u * br;
-                for (uint32_t k = S.brow_ptr[br]; k < S.brow_ptr[br + 1]; ++k) {
-                    const float *B = S.bval + (size_t)k * 36u + a * 6u;
-                    const double *xc = x64 + 6u * (size_t)S.bcol[k];
-#pragma unroll
-                    for (int j = 0; j < 6; ++j) s += (double)B[j] * xc[j];
-                }
-            } else {
-                for (uint32_t k = S.row_ptr[i]; k < S.row_ptr[i + 1]; ++k) s += (double)S.val[k] * x64[S.col[k]];
+        if (S.layout == LAYOUT_BSR6) {
+            if (t < rows) {
+                const uint32_t i = T.row0 + t;
+                const double bi = (double)__ldg(S.b_orig + i);
+                const double r64 = bi - resid_row_bsr6(S, i);
+                bin[i] = (float)r64;
+                rr = r64 * r64;
+                bb = bi * bi;
             }
-            const double bi = (double)S.b_orig[i];
-            const double r64 = bi - s;
-            const_cast<float *>(S.b)[i] = (float)r64;
-            rr = r64 * r64;
-            bb = bi * bi;
+        } else {
+            constexpr uint32_t kLanes = 8, kRowsPerPass = kThreads / kLanes;
+            const uint32_t sub = t / kLanes, l = t % kLanes;
+            const double *__restrict__ x64 = S.x64;
+            for (uint32_t r0 = 0; r0 < rows; r0 += kRowsPerPass) {
+                const uint32_t o = r0 + sub;
+                double sum = 0.0;
+                if (o < rows) {
+                    const uint32_t i = T.row0 + o;
+                    const uint32_t k0 = __ldg(S.row_ptr + i), k1 = __ldg(S.row_ptr + i + 1);
+                    uint32_t k = k0 + l;
+                    for (; k + kLanes < k1; k += 2 * kLanes) {
+                        const float v0 = __ldcs(S.val + k), v1 = __ldcs(S.val + k + kLanes);
+                        const uint32_t c0 = __ldcs(S.col + k), c1 = __ldcs(S.col + k + kLanes);
+                        sum += (double)v0 * x64[c0];
+                        sum += (double)v1 * x64[c1];
+                    }
+                    if (k < k1) sum += (double)__ldcs(S.val + k) * x64[__ldcs(S.col + k)];
+                }
+                sum += __shfl_xor_sync(0xffffffffu, sum, 4);
+                sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+                sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+                if (o < rows && l == 0) {
+                    const uint32_t i = T.row0 + o;
+                    const double bi = (double)__ldg(S.b_orig + i);
+                    const double r64 = bi - sum;
+                    bin[i] = (float)r64;
+                    rr += r64 * r64;
+                    bb += bi * bi;
+                }
+            }
         }
         const double2 tot = block_sum2(rr, bb, red);
         if (t == 0) S.part_b[it.tile] = tot;

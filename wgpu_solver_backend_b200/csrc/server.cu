@@ -32,8 +32,14 @@ struct Request {
     uint64_t id = 0;
     uint32_t n = 0;
     uint64_t nnz = 0;
+    // The request's arrays: copies owned here, or (WSB_SERVER_BORROW_INPUTS)
+    // the caller's arrays, read in place until the request is done. The
+    // pointers below are the ones every stage uses.
     std::vector<uint32_t> row_ptr, col, bs;
     std::vector<float> val, b, x0;
+    const uint32_t *p_row_ptr = nullptr, *p_col = nullptr, *p_bs = nullptr;
+    const float *p_val = nullptr, *p_b = nullptr, *p_x0 = nullptr;
+    uint64_t bs_len = 0;
     SolveCfg cfg;
     bool always_x = false;
     std::vector<double> hist;
@@ -53,7 +59,7 @@ struct Request {
 
 // Device bytes a request holds while resident (matrix, LU, vectors, partials).
 uint64_t estimate_bytes(const Request &r) {
-    const uint64_t n = r.n, nnz = r.nnz, nb = r.bs.size() ? r.bs.size() - 1 : 0;
+    const uint64_t n = r.n, nnz = r.nnz, nb = r.bs_len ? r.bs_len - 1 : 0;
     uint64_t a = 8 * nnz + 4 * (n + 1) + 8 * kPadElems + 8 * (n / 16 + 64);      // CSR (BSR6 is smaller)
     uint64_t m = 144 * nb + 4 * (nb + 1) + 16 * (n / 16 + 64) + 1024;            // LU, starts, tiles
     uint64_t v = 6 * 4 * (n + kPadElems) + 8 * (n / 16 + 64) + 16 * (n / 16 + 64) + 8 * 4096;
@@ -78,6 +84,7 @@ struct wsb_server {
     std::unordered_map<uint64_t, std::unique_ptr<Request>> table;
     uint64_t next_id = 1;
     uint64_t bytes_in_use = 0, bytes_peak = 0;
+    uint32_t uploading = 0;          // requests an uploader is preparing
     wsb_server_stats stats{};
     bool stopping = false;
     std::vector<std::thread> uploaders;
@@ -97,6 +104,8 @@ struct wsb_server {
         r->col.shrink_to_fit();
         r->val.clear();
         r->val.shrink_to_fit();
+        r->p_row_ptr = r->p_col = r->p_bs = nullptr;
+        r->p_val = nullptr;
         if (status == WSB_OK) ++stats.completed;
         else ++stats.failed;
     }
@@ -127,24 +136,43 @@ struct wsb_server {
                 bytes_in_use += need;
                 bytes_peak = std::max(bytes_peak, bytes_in_use);
                 r->state = Request::UPLOADING;
+                ++uploading;
             }
             std::string err;
-            int rc = validate_system(r->n, r->row_ptr.data(), r->col.data(), r->nnz, r->bs.data(), r->bs.size(), &err);
-            std::vector<float> lu;
-            if (!rc) {
-                lu.resize((r->bs.size() - 1) * 36 + 1);
-                rc = build_lu_blocks_6(r->n, r->row_ptr.data(), (uint64_t)r->n + 1, r->col.data(), r->nnz, r->val.data(),
-                                       r->nnz, r->bs.data(), r->bs.size(), lu.data(), &err);
-            }
-            if (!rc) {
+            int rc = WSB_OK;
+            const auto t0 = Clock::now();
+            double prep_ms = 0.0;
+            if (opts.flags & WSB_SERVER_DEVICE_PREP) {
+                // O(n) checks and the tile lists on the host; the column
+                // check, the BSR6 conversion and the LU on the GPU.
                 r->A.reset(new MatA());
                 r->M.reset(new Precond());
-                rc = upload_matA(ctx, r->n, r->row_ptr.data(), r->col.data(), r->val.data(), r->nnz, r->bs.data(),
-                                 r->bs.size(), WSB_LAYOUT_AUTO, upload_stream, r->A.get());
-                if (!rc) rc = upload_precond(ctx, r->n, lu.data(), r->bs.data(), r->bs.size(), upload_stream, r->M.get());
+                rc = prepare_system_device(ctx, r->n, r->p_row_ptr, r->p_col, r->p_val, r->nnz, r->p_bs, r->bs_len,
+                                           WSB_LAYOUT_AUTO, upload_stream, r->A.get(), r->M.get());
                 if (rc) err = thread_error();
+            } else {
+                rc = validate_system(r->n, r->p_row_ptr, r->p_col, r->nnz, r->p_bs, r->bs_len, &err);
+                std::vector<float> lu;
+                if (!rc) {
+                    lu.resize((r->bs_len - 1) * 36 + 1);
+                    rc = build_lu_blocks_6(r->n, r->p_row_ptr, (uint64_t)r->n + 1, r->p_col, r->nnz, r->p_val, r->nnz,
+                                           r->p_bs, r->bs_len, lu.data(), &err);
+                }
+                prep_ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+                if (!rc) {
+                    r->A.reset(new MatA());
+                    r->M.reset(new Precond());
+                    rc = upload_matA(ctx, r->n, r->p_row_ptr, r->p_col, r->p_val, r->nnz, r->p_bs, r->bs_len,
+                                     WSB_LAYOUT_AUTO, upload_stream, r->A.get());
+                    if (!rc) rc = upload_precond(ctx, r->n, lu.data(), r->p_bs, r->bs_len, upload_stream, r->M.get());
+                    if (rc) err = thread_error();
+                }
             }
+            const double all_ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
             std::lock_guard<std::mutex> lk(mu);
+            --uploading;
+            stats.host_prep_ms += prep_ms;
+            stats.upload_ms += all_ms - prep_ms;
             if (rc) {
                 r->A.reset();
                 r->M.reset();
@@ -164,18 +192,25 @@ struct wsb_server {
         cudaSetDevice(ctx->device);
         for (;;) {
             std::vector<Request *> admit;
+            bool more_coming = false;
             {
                 std::unique_lock<std::mutex> lk(mu);
+                const auto tw = Clock::now();
                 cv_sched.wait(lk, [&] { return stopping || !ready.empty() || !active.empty(); });
+                stats.sched_idle_ms += std::chrono::duration<double, std::milli>(Clock::now() - tw).count();
                 if (stopping && active.empty() && ready.empty()) return;
                 while (!ready.empty() && (opts.max_active == 0 || active.size() + admit.size() < opts.max_active)) {
                     admit.push_back(ready.front());
                     ready.pop_front();
                 }
+                // Requests still on their way to the GPU: keep steps short so
+                // they join soon; otherwise longer steps (fewer host turnarounds).
+                more_coming = !queued.empty() || !ready.empty() || uploading > 0;
             }
+            const auto ta = Clock::now();
             for (Request *r : admit) {
                 int rc = eng->add(r->A.get(), r->M.get(), r->cfg, &r->slot);
-                if (!rc) rc = eng->set_rhs(r->slot, r->b.data(), r->x0.data(), false);
+                if (!rc) rc = eng->set_rhs(r->slot, r->p_b, r->p_x0, false);
                 std::lock_guard<std::mutex> lk(mu);
                 if (rc) {
                     r->A.reset();
@@ -189,15 +224,19 @@ struct wsb_server {
                     active.push_back(r);
                 }
             }
+            const double admit_ms = std::chrono::duration<double, std::milli>(Clock::now() - ta).count();
             if (active.empty()) continue;
             const auto t0 = Clock::now();
             bool left = false;
-            int rc = eng->step(opts.iters_per_step, &left);
+            const uint32_t iters = more_coming ? opts.iters_per_step : 4 * opts.iters_per_step;
+            int rc = eng->step(iters, &left);
             const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
             std::vector<Request *> finished;
-            std::lock_guard<std::mutex> lk(mu);
+            std::unique_lock<std::mutex> lk(mu);
+            const auto tr = Clock::now();
             stats.steps += 1;
             stats.busy_ms += ms;
+            stats.admit_ms += admit_ms;
             stats.kernel_launches = eng->launches();
             if (rc) {
                 // A device error ends every active request.
@@ -233,6 +272,7 @@ struct wsb_server {
                 finish(r, st, rc ? fatal : "");
                 active.erase(std::find(active.begin(), active.end(), r));
             }
+            stats.retire_ms += std::chrono::duration<double, std::milli>(Clock::now() - tr).count();
             if (!finished.empty()) {
                 cv_done.notify_all();
                 cv_upload.notify_all();
@@ -281,12 +321,28 @@ extern "C" int wsb_server_submit(wsb_server *s, uint32_t n, const uint32_t *row_
     auto r = std::make_unique<Request>();
     r->n = n;
     r->nnz = nnz;
-    r->row_ptr.assign(row_ptr, row_ptr + (size_t)n + 1);
-    r->col.assign(col, col + nnz);
-    r->val.assign(val, val + nnz);
-    r->bs.assign(bs, bs + bs_len);
-    r->b.assign(b, b + n);
-    r->x0.assign(x0, x0 + n);
+    r->bs_len = bs_len;
+    if (s->opts.flags & WSB_SERVER_BORROW_INPUTS) {
+        r->p_row_ptr = row_ptr;
+        r->p_col = col;
+        r->p_val = val;
+        r->p_bs = bs;
+        r->p_b = b;
+        r->p_x0 = x0;
+    } else {
+        r->row_ptr.assign(row_ptr, row_ptr + (size_t)n + 1);
+        r->col.assign(col, col + nnz);
+        r->val.assign(val, val + nnz);
+        r->bs.assign(bs, bs + bs_len);
+        r->b.assign(b, b + n);
+        r->x0.assign(x0, x0 + n);
+        r->p_row_ptr = r->row_ptr.data();
+        r->p_col = r->col.data();
+        r->p_val = r->val.data();
+        r->p_bs = r->bs.data();
+        r->p_b = r->b.data();
+        r->p_x0 = r->x0.data();
+    }
     SolveCfg c;
     c.max_iter = max_iter;
     c.rel_tol = rel_tol;

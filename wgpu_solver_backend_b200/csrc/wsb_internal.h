@@ -155,6 +155,7 @@ struct StepParams {
     uint32_t error;                    // nonzero: a bounded wait ran out or a work item was invalid
     uint32_t num_sys;                  // entries of the SysDesc array (work items are checked against it)
     uint32_t pad;
+    unsigned long long wait_cycles;    // limit of one pipeline wait in SM clock cycles; 0: the default (~2 s)
 };
 
 // ---------------------------------------------------------------------------
@@ -181,6 +182,7 @@ int fail(Context *ctx, int status, const char *fmt, ...);
 // ---------------------------------------------------------------------------
 struct Context {
     int device = 0;
+    unsigned long long wait_cycles = 0;  // StepParams::wait_cycles of this context's launches (0: default)
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;     // own_stream or the caller's
     cudaDeviceProp prop{};
