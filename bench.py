@@ -294,6 +294,17 @@ def run_reference_plain(args, world, rank, local):
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+# Server configuration of the e2e figure, and the others timed beside it
+# (one burst pass each): borrow_inputs reads the caller's arrays in place
+# instead of copying them at submit; device_prep builds each request's LU
+# (and BSR6 form) on the GPU instead of the host.
+SERVER_VARIANTS = {"copy+host_prep": dict(borrow_inputs=False, device_prep=False),
+                   "borrow+host_prep": dict(borrow_inputs=True, device_prep=False),
+                   "copy+device_prep": dict(borrow_inputs=False, device_prep=True),
+                   "borrow+device_prep": dict(borrow_inputs=True, device_prep=True)}
+SERVER_CFG = SERVER_VARIANTS["borrow+host_prep"]
+
+
 def mixed_kw():
     import wgpu_solver_backend_b200 as wsb
 
@@ -524,9 +535,10 @@ def run_serve(args, world, rank, local):
     R = len(pool)
     n_total = sum(p["n"] for p in pool)
     kw = mixed_kw()
-    srv = wsb.Server(ctx, memory_budget_bytes=120 << 30, iters_per_step=16)
+    srv = wsb.Server(ctx, memory_budget_bytes=120 << 30, iters_per_step=16, **SERVER_CFG)
     for _ in range(args.warmup):
         served_pass(srv, pool[: min(8, R)])
+    st0 = srv.stats()
     barrier(world)
     clocks = ClockSampler(local)
     clocks.start()
@@ -556,6 +568,21 @@ def run_serve(args, world, rank, local):
     mix_ok = sum(1 for r, tg in zip(res_mix, tmix) if r["rc"] == 0 and r["final_relres"] <= tg)
     st = srv.stats()
     srv.close()
+    # Where the server's time goes over the timed burst passes (and the two
+    # passes after them): host preparation and copies in the uploader
+    # threads, the scheduler's engine steps, admissions, retirements, idling.
+    server_phases = {k: st[k] - st0[k] for k in ("busy_ms", "host_prep_ms", "upload_ms", "admit_ms", "retire_ms",
+                                                 "sched_idle_ms", "steps")}
+    # One burst pass of every other server configuration, for comparison.
+    server_variants = {}
+    for name, cfg in SERVER_VARIANTS.items():
+        if cfg == SERVER_CFG:
+            continue
+        sv = wsb.Server(ctx, memory_budget_bytes=120 << 30, iters_per_step=16, **cfg)
+        served_pass(sv, pool[: min(8, R)])
+        mk_v, lat_v, _ = served_pass(sv, pool)
+        sv.close()
+        server_variants[name] = {"solves_per_s": R / mk_v, "burst_p99_ms": float(np.percentile(lat_v, 99))}
     # Resident batch: matrices already in HBM, one batched solve of the set.
     mats = [wsb.Matrix.create(ctx, p["row_ptr"], p["col_idx"], p["values"], p["block_starts"]) for p in pool]
     dev_s, batch_launches = 0.0, 0
@@ -658,7 +685,8 @@ def run_serve(args, world, rank, local):
                                 "solves_per_s": R / mk_mix, "met_target": mix_ok, "of": R,
                                 "p50_ms": float(np.percentile(lat_mix, 50)), "p99_ms": float(np.percentile(lat_mix, 99)),
                                 "path": "continuous-batching server, burst, host arrays"},
-        "server": {"steps": st["steps"], "device_bytes_peak": st["device_bytes_peak"]},
+        "server": {"steps": st["steps"], "device_bytes_peak": st["device_bytes_peak"], "config": SERVER_CFG,
+                   "phases_ms": server_phases, "other_configs_one_pass": server_variants},
         "failures": failures[:20],
         "host_generate_s": t_gen,
         "gpu_launches": batch_launches,

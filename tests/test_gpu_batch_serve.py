@@ -117,3 +117,41 @@ def test_server_overlapping_arrivals(ctx):
         xa, ra = m.solve(s["b"], max_iter=5000, rel_tol=1e-6)
         assert r["rc"] == 0 and r["iterations"] == ra["iterations"]
         assert np.array_equal(x, xa)
+
+
+@pytest.mark.parametrize("borrow,device_prep", [(True, False), (False, True), (True, True)])
+def test_server_borrowed_inputs_and_device_preparation(ctx, borrow, device_prep):
+    """The server's options change where the work happens, not the answers:
+    borrowed inputs (read in place, no copy at submit) and GPU-side
+    preparation (column check, BSR6 conversion and LU on the device) give
+    each request the same iterations and bits as solving it alone, and a
+    request whose first block has a zero pivot fails with the LU message."""
+    systems = _systems()
+    precs = [wsb.PREC_F32_F64DOT, wsb.PREC_MIXED_F64_IR] * 3
+    alone = []
+    for s, p in zip(systems, precs):
+        m = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"])
+        alone.append(m.solve(s["b"], max_iter=5000, rel_tol=1e-8, precision=p, raise_on_error=False))
+    bad = wsb.lattice_generate(3, seed=5)
+    vals = bad["values"].copy()
+    vals[: bad["row_ptr"][6]] = 0.0  # rows 0..5: the first 6x6 block is all zero
+    srv = wsb.Server(ctx, iters_per_step=8, borrow_inputs=borrow, device_prep=device_prep)
+    try:
+        rids = [srv.submit(s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], s["b"], max_iter=5000,
+                           rel_tol=1e-8, precision=p) for s, p in zip(systems, precs)]
+        rbad = srv.submit(bad["row_ptr"], bad["col_idx"], vals, bad["block_starts"], bad["b"], max_iter=100,
+                          rel_tol=1e-8)
+        for i, rid in enumerate(rids):
+            x, r = srv.wait(rid, 120.0)
+            xa, ra = alone[i]
+            assert r["rc"] == ra["rc"] and r["iterations"] == ra["iterations"], (i, r, ra)
+            assert np.array_equal(x.view(np.uint32), xa.view(np.uint32)), i
+        _, r = srv.wait(rbad, 60.0)
+        assert r["rc"] == wsb._lib.ZERO_PIVOT
+        assert "LU zero pivot at k = 0" in ctx.last_error()
+        st = srv.stats()
+        assert st["completed"] == len(systems) and st["failed"] == 1
+        if device_prep:
+            assert st["host_prep_ms"] == 0.0
+    finally:
+        srv.close()

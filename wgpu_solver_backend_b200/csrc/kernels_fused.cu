@@ -161,11 +161,9 @@ __device__ __forceinline__ void mbar_arrive_warp(uint64_t *bar) {
 }
 
 // The pipelined kernels run their consumer threads in the low warps
-// (kSpmvConsumers in the SpMV, kUpdGroups groups of kUpdConsumers /
-// kUpdGroups in the update kernels), then one producer warp (plus the gather
-// warps in the SpMV). Consumers synchronise among themselves on named
-// barriers (1, and 2 for the second update group) so the other warps never
-// have to join. Kernels without a producer warp launch exactly kThreads
+// (kSpmvConsumers in the SpMV, kUpdConsumers in the update kernels), then one
+// producer warp (plus the gather warps in the SpMV). Consumers synchronise
+// among themselves on named barrier 1 so the other warps never have to join. Kernels without a producer warp launch exactly kThreads
 // threads and use barrier 1.
 
 template <int N = kThreads>
@@ -920,59 +918,95 @@ __device__ __forceinline__ float staged_r(const float *stage, uint32_t o, float 
                  : __fadd_rn(stage[2 * kVecCap + o], __fmul_rn(ma, stage[3 * kVecCap + o]));
 }
 
-// z = U^-1 L^-1 r for the blocks starting in the tile (block_jacobi.wgsl:
-// unit-L forward solve lines 93-101, U backward solve dividing by U(i,i)
-// lines 103-122, rows i < m = min(6, len) only, lines 79 and 124-126). One
-// thread per block, in registers. The thread forms its rows' updated r from
-// the stage itself (the same operations as the row update), so the solve
-// does not wait for the other threads. Solved rows are tagged with `tag` in
-// sflag.
+// Block solve of one thread: block blk0 + j of the tile, rows [off, off + m)
+// of the stage (m = min(6, block length)). The thread forms the rows' updated
+// residual from the staged slices itself (loop: r + (-alpha) Ap, init:
+// b - A x0), runs z = U^-1 L^-1 r in registers with the reference's operation
+// order (block_jacobi.wgsl: unit-L forward solve lines 93-101, U backward
+// solve dividing by U(i,i) lines 103-122, rows i < m only, lines 79 and
+// 124-126), and writes its rows' new x (loop), r and z back into the stage
+// (slots 0, 2 and 1; each thread touches only its own rows, after reading
+// them). FP64 r.r (init: b.b) and r.z of the rows go to da and rz.
 template <bool kInit>
-__device__ __forceinline__ void bj_stage(const UpdDesc &d, const float *stage, float *sz, uint32_t *sflag,
-                                         uint32_t tag, uint32_t j) {
-    if (j >= d.nblk) return;
+__device__ __forceinline__ void bj_block(const UpdDesc &d, float *stage, uint32_t j, double &da, double &rz) {
     const uint32_t *bs = reinterpret_cast<const uint32_t *>(stage + kBsOff);
     const uint32_t off = bs[d.blk0 + j - d.ba], nxt = bs[d.blk0 + j + 1 - d.ba];
     const uint32_t m = min(nxt - off, 6u);
     const uint32_t ro = off - d.ra;
     const float ma = -d.alpha;
-    const float *L = stage + kLuOff + j * 36u;
-    const uint32_t lo = off - d.row0;
-    float y[6], xs[6];
+    const float2 *L2 = reinterpret_cast<const float2 *>(stage + kLuOff + j * 36u);
+    float L[36];
+#pragma unroll
+    for (int q = 0; q < 18; ++q) {
+        const float2 v = L2[q];
+        L[2 * q] = v.x;
+        L[2 * q + 1] = v.y;
+    }
+    float rv[6], y[6], xs[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
+        rv[i] = (uint32_t)i < m ? staged_r<kInit>(stage, ro + i, ma) : 0.0f;
         y[i] = 0.0f;
         xs[i] = 0.0f;
     }
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
         if ((uint32_t)i < m) {
-            float s = staged_r<kInit>(stage, ro + i, ma);
+            float t = rv[i];
 #pragma unroll
-            for (int q = 0; q < i; ++q) s = __fsub_rn(s, __fmul_rn(L[i * 6 + q], y[q]));
-            y[i] = s;
+            for (int q = 0; q < i; ++q) t = __fsub_rn(t, __fmul_rn(L[i * 6 + q], y[q]));
+            y[i] = t;
         }
     }
 #pragma unroll
     for (int i = 5; i >= 0; --i) {
         if ((uint32_t)i < m) {
-            float s = y[i];
+            float t = y[i];
 #pragma unroll
             for (int q = i + 1; q < 6; ++q)
-                if ((uint32_t)q < m) s = __fsub_rn(s, __fmul_rn(L[i * 6 + q], xs[q]));
-            xs[i] = __fdiv_rn(s, L[i * 6 + i]);
+                if ((uint32_t)q < m) t = __fsub_rn(t, __fmul_rn(L[i * 6 + q], xs[q]));
+            xs[i] = __fdiv_rn(t, L[i * 6 + i]);
         }
     }
 #pragma unroll
-    for (int i = 0; i < 6; ++i)
+    for (int i = 0; i < 6; ++i) {
         if ((uint32_t)i < m) {
-            sz[lo + i] = xs[i];
-            sflag[lo + i] = tag;
+            const uint32_t o = ro + i;
+            if (kInit) {
+                const float bi = stage[o];
+                da += (double)bi * (double)bi;
+            } else {
+                stage[o] = __fadd_rn(stage[o], __fmul_rn(d.alpha, stage[kVecCap + o]));
+                da += (double)rv[i] * (double)rv[i];
+            }
+            stage[2 * kVecCap + o] = rv[i];
+            stage[kVecCap + o] = xs[i];
+            rz += (double)rv[i] * (double)xs[i];
         }
+    }
 }
 
-// Barrier, reductions and ticket of one consumer group of the update
-// kernels: GT threads (local index lt) on named barrier BAR.
+// A row the block solve leaves alone (position >= 6 in its block): x and r
+// are updated, z keeps its value (read from memory) and enters r.z as it is.
+template <bool kInit>
+__device__ __forceinline__ void passive_row(const UpdDesc &d, float *stage, uint32_t row, double &da, double &rz) {
+    const uint32_t o = row - d.ra;
+    const float ri = staged_r<kInit>(stage, o, -d.alpha);
+    const float zi = d.z[row];
+    if (kInit) {
+        const float bi = stage[o];
+        da += (double)bi * (double)bi;
+    } else {
+        stage[o] = __fadd_rn(stage[o], __fmul_rn(d.alpha, stage[kVecCap + o]));
+        da += (double)ri * (double)ri;
+    }
+    stage[2 * kVecCap + o] = ri;
+    stage[kVecCap + o] = zi;
+    rz += (double)ri * (double)zi;
+}
+
+// Barrier, reductions and ticket of the update consumers: GT threads (local
+// index lt) on named barrier BAR.
 template <int GT, int BAR>
 __device__ __forceinline__ void gsync() {
     asm volatile("bar.sync %0, %1;" ::"n"(BAR), "n"(GT) : "memory");
@@ -1126,8 +1160,8 @@ __device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, St
         if (base + lane * G < nw) it = work[base + lane * G];  // next batch, in flight
         __syncwarp();
         if (lane == 0) {
-            // After the last tile: one end marker for each consumer group.
-            const uint32_t n_out = more ? cnt : cnt + kUpdGroups;
+            // After the last tile: one end marker for the consumers.
+            const uint32_t n_out = more ? cnt : cnt + 1;
             for (uint32_t i = 0; i < n_out; ++i) {
                 const uint32_t s = k % NS;
                 if (k >= NS && !mbar_wait(&empty[s], ((k / NS) - 1) & 1u, lim)) {
@@ -1155,125 +1189,89 @@ __device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, St
     }
 }
 
-// Shared state of one consumer group of the update kernels.
-struct UpdGroupSmem {
-    float sz[kUpdTileRows];
-    uint32_t sflag[kUpdTileRows];
-    double red[64];
-    double2 wred[2 * (kUpdConsumers / kUpdGroups / 32)];
-    int s_last, s_ok[2];
-};
-
-// kInit = false (k_update): x += alpha p; r += (-alpha) Ap; z = M^-1 r; FP64
-// r.r and r.z per tile. kInit = true (k_init, after k_spmv_init):
-// r = b + (-1)(A x0); z = M^-1 r; p = z; FP64 b.b and r.z per tile
-// (compute.rs:226-331). Per-system results are formed by flush_upd.
-// The consumers form kUpdGroups independent groups of GT threads; group G
-// takes tiles G, G + kUpdGroups, ... of the ring (each thread kUpdTileRows /
-// GT rows of a tile), so one group's serial block solves overlap the other
-// group's row updates. Per tile a group passes two barriers of its own: the
-// stage wait (which also separates the previous tile's warp partials from
-// their publication by the group's thread 0) and the one between the block
-// solves and the z writes.
-template <bool kInit, int G>
+// Consumers of the update kernels. kInit = false (k_update): x += alpha p;
+// r += (-alpha) Ap; z = M^-1 r; FP64 r.r and r.z per tile. kInit = true
+// (k_init, after k_spmv_init): r = b + (-1)(A x0); z = M^-1 r; p = z; FP64
+// b.b and r.z per tile (compute.rs:226-331). Per-system results are formed by
+// flush_upd. A tile holds at most NU blocks: consumer j solves block j of the
+// tile (bj_block; its rows >= 6, if any, are passive rows) and the rows in
+// front of the tile's first block start (continuation rows of a long block)
+// are shared out. The new x, r and z go back into the stage, and after one
+// barrier all consumers copy the tile's rows out with consecutive threads on
+// consecutive rows. Per tile the consumers pass two barriers: the stage wait
+// (which also keeps the next tile's warp partials out of wred until thread 0
+// has published this tile's) and the one before the copy-out.
+template <bool kInit>
 __device__ __forceinline__ void upd_consumers(const SysDesc *__restrict__ sys, StepParams *sp, float *smem,
-                                              uint64_t *full, uint64_t *empty, const UpdDesc *desc,
-                                              UpdGroupSmem &g, long long lim) {
+                                              uint64_t *full, uint64_t *empty, const UpdDesc *desc, double *red,
+                                              double2 *wred, int *s_last, int *s_ok, long long lim) {
     constexpr uint32_t NS = kUpdStages;
-    constexpr int GT = NU / kUpdGroups;  // threads of the group
-    constexpr int BAR = 1 + G;           // its named barrier
-    constexpr uint32_t RPT = kUpdTileRows / GT;  // rows per thread
-    const uint32_t lt = threadIdx.x - G * GT;
+    constexpr int BAR = 1;
+    const uint32_t lt = threadIdx.x;
     uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles of run_sys published since the last ticket
-    double2 *pend_part = nullptr;                 // thread 0: partial slot of the tile in wred
-    bool pend = false;
-    uint32_t n = 0;  // tiles this group has taken
-    for (uint32_t k = G;; k += kUpdGroups, ++n) {
+    for (uint32_t k = 0;; ++k) {
         const uint32_t s = k % NS, par = (k / NS) & 1u;
-        if (lt == 0) g.s_ok[n & 1u] = mbar_wait(&full[s], par, lim) ? 1 : 0;
-        gsync<GT, BAR>();
-        if (!g.s_ok[n & 1u]) {
+        if (lt == 0) s_ok[k & 1u] = mbar_wait(&full[s], par, lim) ? 1 : 0;
+        gsync<NU, BAR>();
+        if (!s_ok[k & 1u]) {
             if (lt == 0) atomicOr(&sp->error, kInit ? kErrInitConsumerWait : kErrUpdConsumerWait);
             return;
         }
         mbar_observe(&full[s], par, lim);
-        // The descriptor is read in place: it stays valid until this stage
-        // is handed back; what is needed after that is copied first.
         const UpdDesc &d = desc[s];
-        if (lt == 0 && pend) {
-            const double2 *wr = g.wred + (GT / 32) * ((n - 1) & 1u);
-            double va = 0.0, vb = 0.0;
-#pragma unroll
-            for (int q = 0; q < GT / 32; ++q) {
-                va += wr[q].x;
-                vb += wr[q].y;
-            }
-            *pend_part = make_double2(va, vb);
-            pend = false;
-        }
         if (!d.valid) break;
         if (d.sys != run_sys) {
-            flush_upd<kInit, GT, BAR>(sys, sp, run_sys, run_cnt, g.red, &g.s_last, lt);
+            flush_upd<kInit, NU, BAR>(sys, sp, run_sys, run_cnt, red, s_last, lt);
             run_sys = d.sys;
             run_cnt = 0;
         }
         float *stage = smem + s * kUpdStageFloats;
-        const float ma = -d.alpha;
-        float ri[RPT];
-        double da = 0.0;  // loop: r.r; init: b.b
-#pragma unroll
-        for (uint32_t q = 0; q < RPT; ++q) {
-            const uint32_t t = lt + q * GT;
-            ri[q] = 0.0f;
-            if (t < d.rows) {
-                const uint32_t i = d.row0 + t, o = d.row0 - d.ra + t;
-                ri[q] = staged_r<kInit>(stage, o, ma);
-                if (kInit) {
-                    const float bi = stage[o];
-                    da += (double)bi * (double)bi;
-                } else {
-                    const float xi = __fadd_rn(stage[o], __fmul_rn(d.alpha, stage[kVecCap + o]));
-                    d.x[i] = xi;
-                    da += (double)ri[q] * (double)ri[q];
-                }
-                d.r[i] = ri[q];
-            }
-        }
-        const uint32_t tag = n + 1;
-        bj_stage<kInit>(d, stage, g.sz, g.sflag, tag, lt);
-        const uint32_t rows = d.rows, row0 = d.row0;
-        float *const zv = d.z;
-        float *const pv = d.p;
-        double2 *const part_slot = d.part + d.tile;
-        // Every thread is done reading the stage (it wrote nothing into it):
-        // hand it back to the producer.
-        mbar_arrive_warp(&empty[s]);
-        gsync<GT, BAR>();
-        double rz = 0.0;
-#pragma unroll
-        for (uint32_t q = 0; q < RPT; ++q) {
-            const uint32_t t = lt + q * GT;
-            if (t < rows) {
-                const uint32_t i = row0 + t;
-                float zi;
-                if (g.sflag[t] == tag) {
-                    zi = g.sz[t];
-                    zv[i] = zi;
-                } else {
-                    zi = zv[i];  // a row the block solve leaves alone (position >= 6 in its block)
-                }
-                if (kInit) pv[i] = zi;
-                rz += (double)ri[q] * (double)zi;
-            }
+        double da = 0.0, rz = 0.0;  // loop: r.r and r.z; init: b.b and r.z
+        const uint32_t *bs = reinterpret_cast<const uint32_t *>(stage + kBsOff);
+        const uint32_t row1 = d.row0 + d.rows;
+        // Continuation rows of a long block that started in an earlier tile.
+        const uint32_t lead_end = d.nblk ? bs[d.blk0 - d.ba] : row1;
+        for (uint32_t row = d.row0 + lt; row < lead_end; row += NU) passive_row<kInit>(d, stage, row, da, rz);
+        if (lt < d.nblk) {
+            bj_block<kInit>(d, stage, lt, da, rz);
+            // The block's rows >= 6 inside this tile.
+            const uint32_t off = bs[d.blk0 + lt - d.ba], nxt = bs[d.blk0 + lt + 1 - d.ba];
+            const uint32_t end = min(nxt, row1);
+            for (uint32_t row = off + 6u; row < end; ++row) passive_row<kInit>(d, stage, row, da, rz);
         }
         da = warp_sum(da);
         rz = warp_sum(rz);
-        if ((lt & 31u) == 0) g.wred[(GT / 32) * (n & 1u) + (lt >> 5)] = make_double2(da, rz);
-        pend = true;
-        pend_part = part_slot;
+        if ((lt & 31u) == 0) wred[lt >> 5] = make_double2(da, rz);
+        gsync<NU, BAR>();
+        // Copy-out: x (loop), r and z (init: p = z) of the tile's rows.
+        {
+            const uint32_t o0 = d.row0 - d.ra;
+            float *const xv = d.x, *const rv = d.r, *const zv = d.z, *const pv = d.p;
+            for (uint32_t t = lt; t < d.rows; t += NU) {
+                const uint32_t i = d.row0 + t, o = o0 + t;
+                if (!kInit) xv[i] = stage[o];
+                rv[i] = stage[2 * kVecCap + o];
+                const float zi = stage[kVecCap + o];
+                zv[i] = zi;
+                if (kInit) pv[i] = zi;
+            }
+        }
+        if (lt == 0) {
+            double va = 0.0, vb = 0.0;
+#pragma unroll
+            for (int q = 0; q < NU / 32; ++q) {
+                va += wred[q].x;
+                vb += wred[q].y;
+            }
+            d.part[d.tile] = make_double2(va, vb);
+        }
+        // The consumers wrote into the stage: order those writes before the
+        // bulk copies that will next fill it, then hand it back.
+        fence_proxy_async();
+        mbar_arrive_warp(&empty[s]);
         ++run_cnt;
     }
-    if (run_sys != 0xffffffffu) flush_upd<kInit, GT, BAR>(sys, sp, run_sys, run_cnt, g.red, &g.s_last, lt);
+    if (run_sys != 0xffffffffu) flush_upd<kInit, NU, BAR>(sys, sp, run_sys, run_cnt, red, s_last, lt);
 }
 
 template <bool kInit>
@@ -1282,17 +1280,17 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
     __shared__ __align__(8) uint64_t full[NS], empty[NS];
     __shared__ UpdDesc desc[NS];
     __shared__ UpdDesc bdesc[32];
-    __shared__ UpdGroupSmem gsm[kUpdGroups];
+    __shared__ double red[64];
+    __shared__ double2 wred[NU / 32];
+    __shared__ int s_last, s_ok[2];
     const uint32_t tid = threadIdx.x;
     if (tid == 0) {
         for (uint32_t i = 0; i < NS; ++i) {
             mbar_init(&full[i], 1);
-            mbar_init(&empty[i], NU / kUpdGroups / 32);  // the warps of the one group that takes the stage
+            mbar_init(&empty[i], NU / 32);  // one arrival per consumer warp
         }
         fence_barrier_init();
     }
-    for (uint32_t i = tid; i < (uint32_t)kUpdGroups * kUpdTileRows; i += blockDim.x)
-        gsm[i / kUpdTileRows].sflag[i % kUpdTileRows] = 0u;
     __syncthreads();
     pdl_start();
     const long long lim = wait_limit(sp);
@@ -1300,11 +1298,7 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
         if (tid < NU + 32) upd_producer<kInit>(sys, sp, smem, full, empty, desc, bdesc, lim);
         return;
     }
-    const uint32_t grp = tid / (NU / kUpdGroups);
-    if (grp == 0) upd_consumers<kInit, 0>(sys, sp, smem, full, empty, desc, gsm[0], lim);
-    if constexpr (kUpdGroups > 1) {
-        if (grp == 1) upd_consumers<kInit, 1>(sys, sp, smem, full, empty, desc, gsm[1], lim);
-    }
+    upd_consumers<kInit>(sys, sp, smem, full, empty, desc, red, wred, &s_last, s_ok, lim);
 }
 
 }  // namespace
@@ -1412,7 +1406,7 @@ __global__ void k_loop_gate(StepParams *sp, cudaGraphConditionalHandle h) {
 // Mixed precision (FP64 outer iterative refinement).
 // k_resid64: r64 = b - A x64 with FP32 matrix entries and FP64 accumulation;
 // the inner right-hand side becomes (float) r64; FP64 ||r64||^2 and ||b||^2.
-// One work item is one update tile (<= 256 rows). BSR6: one thread per row,
+// One work item is one update tile (kUpdTileRows rows at most). BSR6: one thread per row,
 // which walks its block row four blocks at a time with every load of the four
 // issued before the first multiply (block columns, then 3 float2 of the row's
 // block values and 3 double2 of x64 per block). CSR: eight lanes per row,
@@ -1476,13 +1470,13 @@ __global__ void __launch_bounds__(kThreads) k_resid64(const SysDesc *__restrict_
         float *const bin = const_cast<float *>(S.b);
         double rr = 0.0, bb = 0.0;
         if (S.layout == LAYOUT_BSR6) {
-            if (t < rows) {
-                const uint32_t i = T.row0 + t;
+            for (uint32_t o = t; o < rows; o += kThreads) {
+                const uint32_t i = T.row0 + o;
                 const double bi = (double)__ldg(S.b_orig + i);
                 const double r64 = bi - resid_row_bsr6(S, i);
                 bin[i] = (float)r64;
-                rr = r64 * r64;
-                bb = bi * bi;
+                rr += r64 * r64;
+                bb += bi * bi;
             }
         } else {
             constexpr uint32_t kLanes = 8, kRowsPerPass = kThreads / kLanes;
@@ -1548,8 +1542,7 @@ __global__ void __launch_bounds__(kThreads) k_refine(const SysDesc *__restrict__
         }
         const SysDesc &S = sys[it.sys];
         const UpdTile T = S.utiles[it.tile];
-        if (threadIdx.x < T.row1 - T.row0) {
-            const uint32_t i = T.row0 + threadIdx.x;
+        for (uint32_t i = T.row0 + threadIdx.x; i < T.row1; i += kThreads) {
             S.x64[i] += (double)S.x[i];
             S.x[i] = 0.0f;
         }
@@ -1568,10 +1561,7 @@ __global__ void __launch_bounds__(kThreads) k_x64_to_x32(const SysDesc *__restri
         }
         const SysDesc &S = sys[it.sys];
         const UpdTile T = S.utiles[it.tile];
-        if (threadIdx.x < T.row1 - T.row0) {
-            const uint32_t i = T.row0 + threadIdx.x;
-            S.x[i] = (float)S.x64[i];
-        }
+        for (uint32_t i = T.row0 + threadIdx.x; i < T.row1; i += kThreads) S.x[i] = (float)S.x64[i];
     }
 }
 

@@ -38,7 +38,7 @@ constexpr int kUpdStageFloats = ((4 * (kUpdTileRows + 8) + kUpdBlocks * 36 + kUp
 constexpr int kGatherWarps = WSB_GATHER_WARPS;
 constexpr int kUpdThreads = kUpdConsumers + 32;
 #ifndef WSB_UPD_MIN_CTAS
-#define WSB_UPD_MIN_CTAS 4
+#define WSB_UPD_MIN_CTAS 3
 #endif
 constexpr int kUpdMinCtas = WSB_UPD_MIN_CTAS;
 constexpr int kSpmvThreads = kSpmvConsumers + 32 + 32 * kGatherWarps;

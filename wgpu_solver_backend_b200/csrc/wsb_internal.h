@@ -32,31 +32,24 @@ namespace wsb {
 #define WSB_SPMV_STAGES 2
 #endif
 #ifndef WSB_UPD_STAGES
-#define WSB_UPD_STAGES 3
+#define WSB_UPD_STAGES 4
 #endif
 #ifndef WSB_SPMV_CONSUMERS
 #define WSB_SPMV_CONSUMERS 128
 #endif
 #ifndef WSB_UPD_CONSUMERS
-#define WSB_UPD_CONSUMERS 256
-#endif
-#ifndef WSB_UPD_BLOCKS
-#define WSB_UPD_BLOCKS 64
-#endif
-#ifndef WSB_UPD_GROUPS
-#define WSB_UPD_GROUPS 2
+#define WSB_UPD_CONSUMERS 64
 #endif
 constexpr int kThreads = 256;        // threads per CTA of the vector and refinement kernels
 constexpr int kUpdConsumers = WSB_UPD_CONSUMERS;   // consumer threads per CTA of the update kernels
-constexpr int kUpdTileRows = kUpdConsumers;        // rows per update tile (<= kThreads)
-constexpr int kUpdGroups = WSB_UPD_GROUPS;         // independent consumer groups per update CTA (1 or 2)
-static_assert(kUpdGroups == 1 || kUpdGroups == 2, "update consumer groups");
+static_assert(kUpdConsumers % 32 == 0 && kUpdConsumers <= 1024, "update consumers");
+constexpr int kUpdTileRows = 6 * kUpdConsumers;    // rows per update tile (6 per block)
 constexpr int kSpmvConsumers = WSB_SPMV_CONSUMERS;  // consumer threads per CTA of the SpMV kernels
 constexpr int kSpmvTileRows = kSpmvConsumers;       // rows (or block rows x 6) per SpMV tile
 constexpr int kCsrCap = WSB_CSR_CAP;         // CSR nonzeros per SpMV tile (one TMA stage)
 constexpr int kBsrCapBlocks = WSB_BSR_CAP;   // BSR 6x6 blocks per SpMV tile (144 B each)
 constexpr int kSpmvStages = WSB_SPMV_STAGES; // depth of the SpMV shared-memory ring
-constexpr int kUpdBlocks = WSB_UPD_BLOCKS;         // block-Jacobi blocks per update tile
+constexpr int kUpdBlocks = kUpdConsumers;          // block-Jacobi blocks per update tile (one per consumer)
 constexpr int kUpdStages = WSB_UPD_STAGES;   // depth of the update shared-memory ring
 static_assert(kCsrCap % 4 == 0 && kBsrCapBlocks % 4 == 0 && kSpmvStages >= 2, "SpMV tile caps");
 constexpr int kChunkRows = 4096;     // rows per work item of the vector kernels
