@@ -61,6 +61,8 @@ def lib():
                                       _f32p, C.c_uint64, C.c_float, C.c_float, _u64p, _f32p, _ip]
         L.orc_pcg_f64dot.argtypes = [C.c_uint32, _u32p, _u32p, _f32p, C.c_uint32, _f32p, _u32p, _f32p,
                                      _f32p, C.c_uint64, C.c_float, C.c_float, _u64p, _f64p, _ip]
+        L.orc_pcg_single_reduction_f64dot.argtypes = [C.c_uint32, _u32p, _u32p, _f32p, C.c_uint32, _f32p, _u32p,
+                                                      _f32p, _f32p, C.c_uint64, C.c_float, C.c_float, _u64p, _f64p]
         L.orc_pcg_f64.argtypes = [C.c_uint32, _u32p, _u32p, _f32p, C.c_uint32, _u32p, _f64p, _f64p,
                                   C.c_uint64, C.c_double, _u64p]
         L.orc_true_relres_f64.argtypes = [C.c_uint32, _u32p, _u32p, _f32p, _f32p, _f32p, _f64p]
@@ -174,6 +176,22 @@ def pcg_f64dot(row_ptr, col_idx, values, lu, block_starts, b, x0, max_iter, rel_
                               _p(x, _f32p), int(max_iter), np.float32(rel_tol), np.float32(abs_tol),
                               C.byref(it), _p(hist, _f64p), C.byref(bk))
     return dict(status=st, iterations=it.value, x=x, history=hist[: it.value], breakdown=bk.value)
+
+
+def pcg_single_reduction_f64dot(row_ptr, col_idx, values, lu, block_starts, b, x0, max_iter, rel_tol, abs_tol):
+    """The single-reduction (Chronopoulos-Gear) PCG recurrence with the
+    product's arithmetic. Returns dict(status, iterations, x, history)."""
+    n = len(row_ptr) - 1
+    bs = _u32(block_starts)
+    x = _f32(x0).copy()
+    hist = np.zeros(max(int(max_iter), 1), np.float64)
+    it = C.c_uint64(0)
+    st = lib().orc_pcg_single_reduction_f64dot(n, _p(_u32(row_ptr), _u32p), _p(_u32(col_idx), _u32p),
+                                               _p(_f32(values), _f32p), max(len(bs) - 1, 0), _p(_f32(lu), _f32p),
+                                               _p(bs, _u32p), _p(_f32(b), _f32p), _p(x, _f32p), int(max_iter),
+                                               np.float32(rel_tol), np.float32(abs_tol), C.byref(it),
+                                               _p(hist, _f64p))
+    return dict(status=st, iterations=it.value, x=x, history=hist[: it.value])
 
 
 def pcg_f64(row_ptr, col_idx, values, block_starts, b, x0=None, max_iter=100000, rel_tol=1e-12):

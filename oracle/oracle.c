@@ -365,6 +365,85 @@ int orc_pcg_f64dot(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, con
     return status;
 }
 
+/* M applied with rows >= 6 of a longer block set to 0 (the values the
+ * reference's apply leaves in its zero-initialised z for those rows). */
+static void orc_bj_zero_tail(uint32_t n, uint32_t nb, const float *lu, const uint32_t *bs, const float *in,
+                             float *out)
+{
+    memset(out, 0, sizeof(float) * n);
+    orc_block_jacobi_apply(n, nb, lu, bs, in, out);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Single-reduction PCG of Chronopoulos & Gear (J. Comput. Appl. Math. 25     */
+/* (1989)): u = M r and w = A u are formed explicitly every iteration, s = A p */
+/* by recurrence, and both dots of an iteration, (r, u) and (w, u), come      */
+/* from the same pass. Arithmetic as orc_pcg_f64dot (FP32 vectors, FP64 dots */
+/* and scalars, alpha/beta rounded to f32 where they scale f32 vectors), M as */
+/* orc_block_jacobi_apply with rows >= 6 of a longer block set to 0.         */
+/* ------------------------------------------------------------------------- */
+int orc_pcg_single_reduction_f64dot(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, const float *val,
+                                    uint32_t nb, const float *lu, const uint32_t *bs, const float *b, float *x,
+                                    uint64_t max_iter, float rel_tol, float abs_tol, uint64_t *iters_out,
+                                    double *history)
+{
+    if (iters_out) *iters_out = 0;
+    double bb = dot_f64(n, b, b);
+    if (bb == 0.0) return ORC_OK;
+    double rel2 = (double)rel_tol * (double)rel_tol, abs2 = (double)abs_tol * (double)abs_tol;
+    size_t nn = n ? n : 1;
+    float *v[7];
+    for (int k = 0; k < 7; ++k) {
+        v[k] = (float *)calloc(nn, sizeof(float));
+        if (!v[k]) {
+            for (int j = 0; j < k; ++j) free(v[j]);
+            return ORC_NO_MEMORY;
+        }
+    }
+    float *xg = v[0], *r = v[1], *u = v[2], *w = v[3], *p = v[4], *s = v[5], *tmp = v[6];
+    memcpy(xg, x, sizeof(float) * n);
+    orc_spmv_csr(n, row_ptr, col, val, xg, tmp);
+    for (uint32_t i = 0; i < n; ++i) r[i] = b[i] + (-1.0f) * tmp[i];
+    orc_bj_zero_tail(n, nb, lu, bs, r, u);
+    orc_spmv_csr(n, row_ptr, col, val, u, w);
+    double gamma = dot_f64(n, r, u), delta = dot_f64(n, w, u);
+    int status = ORC_MAXITER;
+    if (max_iter == 0) goto done;
+    if (delta == 0.0) { status = ORC_BREAKDOWN; goto done; }
+    double alpha = gamma / delta, beta = 0.0;
+    for (uint64_t k = 0; k < max_iter; ++k) {
+        float af = (float)alpha, bf = (float)beta, maf = -af;
+#pragma omp parallel for schedule(static) if (n >= ORC_PAR_MIN)
+        for (int64_t i = 0; i < (int64_t)n; ++i) {
+            float pi = u[i] + bf * p[i], si = w[i] + bf * s[i];
+            p[i] = pi;
+            s[i] = si;
+            xg[i] = xg[i] + af * pi;
+            r[i] = r[i] + maf * si;
+        }
+        double rr = dot_f64(n, r, r);
+        if (history) history[k] = rr;
+        if (iters_out) *iters_out = k + 1;
+        if (rr <= abs2 || rr <= rel2 * bb) {
+            memcpy(x, xg, sizeof(float) * n);
+            status = ORC_OK;
+            break;
+        }
+        orc_bj_zero_tail(n, nb, lu, bs, r, u);
+        orc_spmv_csr(n, row_ptr, col, val, u, w);
+        double g2 = dot_f64(n, r, u), d2 = dot_f64(n, w, u);
+        if (gamma == 0.0) { status = ORC_BREAKDOWN; break; }
+        beta = g2 / gamma;
+        double den = d2 - beta * g2 / alpha;
+        if (den == 0.0) { status = ORC_BREAKDOWN; break; }
+        alpha = g2 / den;
+        gamma = g2;
+    }
+done:
+    for (int k = 0; k < 7; ++k) free(v[k]);
+    return status;
+}
+
 /* ------------------------------------------------------------------------- */
 /* Full FP64 block-Jacobi PCG: FP32 matrix entries widened to FP64, block    */
 /* LU recomputed in FP64 with the same no-pivot algorithm (compute.rs:37-71, */

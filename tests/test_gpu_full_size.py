@@ -150,4 +150,8 @@ def test_c3_anisotropic_80cubed_refines_to_1e10_against_the_fp64_oracle(ctx):
     print(f"C3: sweeps={r['refine_sweeps']} iterations={r['iterations']} true_relres={tr:.3e} "
           f"err_vs_fp64_oracle={err:.3e}")
     assert tr <= 1e-10, tr
-    assert err <= 1e-6, err
+    # The same refinement on the CPU (oracle FP32-vector PCG with FP64 dots as
+    # the inner solve) takes 4 sweeps to 1.1e-12 with an error of 2.6e-12
+    # against the FP64 oracle on these rows; the bound leaves a factor of 100
+    # over the residual target for the system's conditioning.
+    assert err <= 1e-8, err

@@ -24,8 +24,8 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import (LAYOUT_AUTO, LAYOUT_BSR6, LAYOUT_CSR, PREC_F32_F64DOT, PREC_MIXED_F64_IR, PREC_REFERENCE_F32,
-                   MatrixInfo, ServerOpts, ServerStats, SolveOpts, SolveResult)
+from ._lib import (LAYOUT_AUTO, LAYOUT_BSR6, LAYOUT_CSR, PREC_F32_F64DOT, PREC_MIXED_F64_IR,
+                   PREC_REFERENCE_F32, MatrixInfo, ServerOpts, ServerStats, SolveOpts, SolveResult)
 
 __all__ = ["WsbError", "GpuBackend", "GpuContext", "GpuBuffer", "SpmvExecutor", "DotScalarExecutor",
            "VecOpsExecutor", "BlockJacobiExecutor", "PcgUpdateScalarsExecutor", "lu_factor_inplace_6",

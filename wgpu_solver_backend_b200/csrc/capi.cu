@@ -797,6 +797,8 @@ static int matrix_solve(wsb_context *ctx, wsb_matrix *m, const float *b, float *
     if (!m) return fail(ctx, WSB_ERR_BAD_INPUT, "matrix is null");
     if (m->A.n && (!b || !x)) return fail(ctx, WSB_ERR_BAD_INPUT, "b and x must not be null");
     const SolveCfg cfg = make_cfg(max_iter, rel, abs_tol, o);
+    if (cfg.precision < WSB_PREC_F32_F64DOT || cfg.precision > WSB_PREC_MIXED_F64_IR)
+        return fail(ctx, WSB_ERR_BAD_INPUT, "unknown precision %d", cfg.precision);
     if (cfg.precision == WSB_PREC_REFERENCE_F32) {
         const auto t0 = std::chrono::steady_clock::now();
         SolveOutcome out;
@@ -955,7 +957,7 @@ extern "C" int wsb_batch_add(wsb_batch *bt, wsb_matrix *m, const float *b, const
     CHECK_CTX(ctx);
     if (!m || (m->A.n && (!b || !x0))) return fail(ctx, WSB_ERR_BAD_INPUT, "bad arguments");
     SolveCfg cfg = make_cfg(max_iter, rel, abs_tol, o);
-    if (cfg.precision == WSB_PREC_REFERENCE_F32)
+    if (cfg.precision != WSB_PREC_F32_F64DOT && cfg.precision != WSB_PREC_MIXED_F64_IR)
         return fail(ctx, WSB_ERR_UNSUPPORTED, "batched solves use FP64 reductions (F32_F64DOT or MIXED_F64_IR)");
     uint32_t slot;
     int rc = bt->eng->add(&m->A, &m->M, cfg, &slot);

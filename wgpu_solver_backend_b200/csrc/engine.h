@@ -95,6 +95,7 @@ struct SolveOutcome {
     double bb = 0.0, rr = 0.0, relres = 0.0;
 };
 
+
 // Multi-system PCG engine. Systems are slots; each owns its Krylov vectors,
 // partial buffers and state in HBM. run()/step() iterate all active slots
 // together with one captured graph: a gate kernel, then a while loop of

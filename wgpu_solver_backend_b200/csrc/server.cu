@@ -316,7 +316,7 @@ extern "C" int wsb_server_submit(wsb_server *s, uint32_t n, const uint32_t *row_
     if (!s || !id) return fail(nullptr, WSB_ERR_BAD_INPUT, "bad arguments");
     if (!row_ptr || (nnz && (!col || !val)) || !bs || bs_len < 1 || (n && (!b || !x0)))
         return fail(s->ctx, WSB_ERR_BAD_INPUT, "null array");
-    if (o && o->precision == WSB_PREC_REFERENCE_F32)
+    if (o && o->precision != WSB_PREC_F32_F64DOT && o->precision != WSB_PREC_MIXED_F64_IR)
         return fail(s->ctx, WSB_ERR_UNSUPPORTED, "the server uses FP64 reductions (F32_F64DOT or MIXED_F64_IR)");
     auto r = std::make_unique<Request>();
     r->n = n;
