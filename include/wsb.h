@@ -195,6 +195,23 @@ typedef enum wsb_layout {
     WSB_LAYOUT_BSR6 = 2
 } wsb_layout;
 
+/* The PCG recurrence (wsb_solve_opts.algorithm). No counterpart in the
+ * reference, which has the classic one only. */
+typedef enum wsb_algorithm {
+    /* The reference's recurrence (compute.rs:336-489): SpMV of p, then x, r and
+     * z = M r, then p = z + beta p; three fused kernels per iteration. */
+    WSB_ALG_CLASSIC = 0,
+    /* The single-reduction recurrence of Chronopoulos and Gear (J. Comput.
+     * Appl. Math. 25, 1989): w = A u with u = M r, s = A p kept by recurrence,
+     * and the iteration's two dots, (r, u) and (A u, u), formed in the update
+     * and SpMV epilogues; the direction update moves into the update kernel,
+     * so an iteration is two fused kernels. Same stop test on the recursive
+     * residual; iterates agree with the classic ones to rounding. FP64
+     * reductions only (F32_F64DOT and MIXED_F64_IR); systems solved together
+     * (a batch, a server) all use one recurrence. */
+    WSB_ALG_SINGLE_REDUCTION = 1
+} wsb_algorithm;
+
 typedef struct wsb_solve_opts {
     uint32_t struct_size;        /* sizeof(wsb_solve_opts) */
     int32_t precision;           /* wsb_precision */
@@ -204,7 +221,7 @@ typedef struct wsb_solve_opts {
     uint64_t history_capacity;   /* entries available in history_out */
     double *history_out;         /* r.r after each PCG iteration (host memory), or NULL */
     int32_t always_write_x;      /* 0: x written only on success, as compute.rs:482-484 */
-    int32_t reserved;
+    int32_t algorithm;           /* wsb_algorithm; default WSB_ALG_CLASSIC */
     double *x64_out;             /* MIXED: receives the FP64 solution (n doubles, host), or NULL.
                                     For server requests it is filled by wsb_server_poll/wait. */
 } wsb_solve_opts;

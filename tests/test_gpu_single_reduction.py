@@ -1,0 +1,83 @@
+"""The single-reduction recurrence (WSB_ALG_SINGLE_REDUCTION, opt-in).
+
+Chronopoulos and Gear's PCG forms u = M r and w = A u explicitly and keeps
+s = A p by recurrence, so the direction update p = u + beta p moves into the
+update kernel and an iteration is two fused kernels instead of three. The
+checks: it agrees with the oracle's statement of the same recurrence
+(orc_pcg_single_reduction_f64dot: same iteration count within 1, solution
+within 1e-5 relative), with the classic product path (iterations within 2 %,
+solution within 1e-5 relative), passes the datasets' compare-x gates, gives
+each system the same bits alone and batched, and carries FP64 refinement to a
+true relative residual of 1e-10.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import wgpu_solver_backend_b200 as wsb
+from conftest import COMPARE_X_GATES, DATASET_SOLVE, load_case
+
+pytestmark = pytest.mark.gpu
+SR = dict(algorithm=wsb.ALG_SINGLE_REDUCTION)
+
+
+def rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("side,aniso,layout", [(10, 0.0, wsb.LAYOUT_BSR6), (10, 0.0, wsb.LAYOUT_CSR),
+                                               (14, 2.0, wsb.LAYOUT_BSR6)])
+def test_single_reduction_matches_its_oracle_and_the_classic_path(ctx, side, aniso, layout):
+    s = wsb.lattice_generate(side, seed=31, aniso_log10=aniso)
+    m = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], layout=layout)
+    x, r = m.solve(s["b"], max_iter=20000, rel_tol=1e-6, **SR)
+    xc, rc = m.solve(s["b"], max_iter=20000, rel_tol=1e-6)
+    lu = wsb.build_lu_blocks_from_csr_block_starts_6(s["n"], s["row_ptr"], s["col_idx"], s["values"],
+                                                     s["block_starts"])
+    o = oracle.pcg_single_reduction_f64dot(s["row_ptr"], s["col_idx"], s["values"], lu, s["block_starts"], s["b"],
+                                           np.zeros(s["n"], np.float32), 20000, 1e-6, 0.0)
+    assert r["rc"] == 0 and o["status"] == oracle.OK
+    assert abs(int(r["iterations"]) - int(o["iterations"])) <= 1, (r["iterations"], o["iterations"])
+    assert rel(x, o["x"]) <= 1e-5, rel(x, o["x"])
+    assert abs(int(r["iterations"]) - int(rc["iterations"])) <= max(1, 0.02 * int(rc["iterations"]))
+    assert rel(x, xc) <= 1e-5, rel(x, xc)
+
+
+@pytest.mark.parametrize("k", [1, 2, 3])
+def test_single_reduction_passes_the_dataset_gates(ctx, k):
+    case, x_ref, _ = load_case(k)
+    a = case.a
+    m = wsb.Matrix.create(ctx, a.row_ptr, a.col_idx, a.values, case.block_starts)
+    x, r = m.solve(case.b, case.x0, **DATASET_SOLVE, **SR)
+    assert r["rc"] == 0
+    st = oracle.compare_x(x_ref, x)
+    rt, at = COMPARE_X_GATES[k]
+    assert st["rel_l2"] <= rt or st["rmse"] <= at, st
+
+
+def test_single_reduction_batch_equals_alone_and_refines(ctx):
+    systems = [wsb.lattice_generate(side, seed=300 + side, aniso_log10=1.0) for side in (4, 9, 6, 12, 5)]
+    mats = [wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"]) for s in systems]
+    precs = [wsb.PREC_F32_F64DOT, wsb.PREC_MIXED_F64_IR, wsb.PREC_F32_F64DOT, wsb.PREC_MIXED_F64_IR,
+             wsb.PREC_F32_F64DOT]
+    alone = [m.solve(s["b"], max_iter=20000, rel_tol=1e-8, precision=p, target_relres=1e-10, **SR)
+             for m, s, p in zip(mats, systems, precs)]
+    bt = wsb.Batch(ctx)
+    ids = [bt.add(m, s["b"], max_iter=20000, rel_tol=1e-8, precision=p, target_relres=1e-10, **SR)
+           for m, s, p in zip(mats, systems, precs)]
+    bt.solve()
+    for i, (s, p) in enumerate(zip(systems, precs)):
+        x, r = bt.result(ids[i], s["n"])
+        xa, ra = alone[i]
+        assert r["rc"] == 0 and r["iterations"] == ra["iterations"], (i, r, ra)
+        assert np.array_equal(x.view(np.uint32), xa.view(np.uint32)), i
+        if p == wsb.PREC_MIXED_F64_IR:
+            assert oracle.true_relres_f64(s["row_ptr"], s["col_idx"], s["values"], s["b"], x.astype(np.float64)) \
+                <= 1e-6  # x is the FP32 rounding of the FP64 solution
+            assert r["final_relres"] <= 1e-10
+    # One recurrence per batch: a classic system cannot join a single-reduction batch.
+    with pytest.raises(wsb.WsbError):
+        bt2 = wsb.Batch(ctx)
+        bt2.add(mats[0], systems[0]["b"], max_iter=100, rel_tol=1e-8, **SR)
+        bt2.add(mats[1], systems[1]["b"], max_iter=100, rel_tol=1e-8)

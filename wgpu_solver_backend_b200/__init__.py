@@ -24,14 +24,14 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import (LAYOUT_AUTO, LAYOUT_BSR6, LAYOUT_CSR, PREC_F32_F64DOT, PREC_MIXED_F64_IR,
-                   PREC_REFERENCE_F32, MatrixInfo, ServerOpts, ServerStats, SolveOpts, SolveResult)
+from ._lib import (ALG_CLASSIC, ALG_SINGLE_REDUCTION, LAYOUT_AUTO, LAYOUT_BSR6, LAYOUT_CSR, PREC_F32_F64DOT,
+                   PREC_MIXED_F64_IR, PREC_REFERENCE_F32, MatrixInfo, ServerOpts, ServerStats, SolveOpts, SolveResult)
 
 __all__ = ["WsbError", "GpuBackend", "GpuContext", "GpuBuffer", "SpmvExecutor", "DotScalarExecutor",
            "VecOpsExecutor", "BlockJacobiExecutor", "PcgUpdateScalarsExecutor", "lu_factor_inplace_6",
            "build_lu_blocks_from_csr_block_starts_6", "pcg_block_jacobi_csr_wgpu", "Matrix", "Batch", "Server",
            "lattice_sizes", "lattice_generate", "PREC_F32_F64DOT", "PREC_REFERENCE_F32", "PREC_MIXED_F64_IR",
-           "LAYOUT_AUTO", "LAYOUT_CSR", "LAYOUT_BSR6"]
+           "LAYOUT_AUTO", "LAYOUT_CSR", "LAYOUT_BSR6", "ALG_CLASSIC", "ALG_SINGLE_REDUCTION"]
 
 
 class WsbError(RuntimeError):
@@ -308,10 +308,12 @@ def build_lu_blocks_from_csr_block_starts_6(n, row_ptr, col_idx, values, block_s
 
 
 def _opts(precision, history_capacity, always_write_x, target_relres=None, inner_rel_tol=None, max_refine=None,
-          x64_out=None):
+          x64_out=None, algorithm=None):
     o = SolveOpts()
     _lib_handle().wsb_solve_opts_default(C.byref(o))
     o.precision = precision
+    if algorithm is not None:
+        o.algorithm = int(algorithm)
     hist = None
     if history_capacity:
         hist = np.zeros(int(history_capacity), np.float64)

@@ -19,6 +19,7 @@ STATUS_NAMES = {0: "OK", 1: "BAD_INPUT", 2: "ZERO_PIVOT", 3: "BREAKDOWN", 4: "NO
                 6: "OUT_OF_MEMORY", 7: "TIMEOUT", 8: "NO_DEVICE", 9: "UNSUPPORTED", 10: "PENDING"}
 
 PREC_F32_F64DOT, PREC_REFERENCE_F32, PREC_MIXED_F64_IR = 0, 1, 2
+ALG_CLASSIC, ALG_SINGLE_REDUCTION = 0, 1
 LAYOUT_AUTO, LAYOUT_CSR, LAYOUT_BSR6 = 0, 1, 2
 
 
@@ -31,7 +32,7 @@ class AdapterInfo(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("precision", C.c_int32), ("target_relres", C.c_double),
                 ("inner_rel_tol", C.c_float), ("max_refine", C.c_uint32), ("history_capacity", C.c_uint64),
-                ("history_out", f64p), ("always_write_x", C.c_int32), ("reserved", C.c_int32), ("x64_out", f64p)]
+                ("history_out", f64p), ("always_write_x", C.c_int32), ("algorithm", C.c_int32), ("x64_out", f64p)]
 
 
 class SolveResult(C.Structure):

@@ -607,12 +607,14 @@ static SolveCfg make_cfg(uint64_t max_iter, float rel, float abs_tol, const wsb_
         if (o->inner_rel_tol > 0) c.inner_rel_tol = o->inner_rel_tol;
         if (o->max_refine > 0) c.max_refine = o->max_refine;
         c.hist_cap = o->history_out ? o->history_capacity : 0;
+        c.algorithm = o->algorithm;
     }
     return c;
 }
 
 static bool same_layout(const SolveCfg &a, const SolveCfg &b) {
     return (a.precision == WSB_PREC_MIXED_F64_IR) == (b.precision == WSB_PREC_MIXED_F64_IR) &&
+           a.algorithm == b.algorithm &&
            std::min<uint64_t>(a.hist_cap, std::max<uint64_t>(a.max_iter, 1)) ==
                std::min<uint64_t>(b.hist_cap, std::max<uint64_t>(b.max_iter, 1));
 }
@@ -799,6 +801,8 @@ static int matrix_solve(wsb_context *ctx, wsb_matrix *m, const float *b, float *
     const SolveCfg cfg = make_cfg(max_iter, rel, abs_tol, o);
     if (cfg.precision < WSB_PREC_F32_F64DOT || cfg.precision > WSB_PREC_MIXED_F64_IR)
         return fail(ctx, WSB_ERR_BAD_INPUT, "unknown precision %d", cfg.precision);
+    if (cfg.precision == WSB_PREC_REFERENCE_F32 && cfg.algorithm != WSB_ALG_CLASSIC)
+        return fail(ctx, WSB_ERR_BAD_INPUT, "reference arithmetic runs the reference's classic recurrence only");
     if (cfg.precision == WSB_PREC_REFERENCE_F32) {
         const auto t0 = std::chrono::steady_clock::now();
         SolveOutcome out;

@@ -148,6 +148,7 @@ struct Engine::Slot {
     void *mem = nullptr;
     size_t mem_bytes = 0;
     float *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *ap = nullptr, *b_orig = nullptr;
+    float *s = nullptr;  // single reduction: s = A p
     double *x64 = nullptr, *part_a = nullptr, *hist = nullptr;
     double2 *part_b = nullptr;
     uint64_t hist_cap = 0;
@@ -167,11 +168,14 @@ Engine::Engine(Context *ctx, cudaStream_t stream) : ctx_(ctx), stream_(stream) {
     cudaFuncSetAttribute(k_spmv_init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpmvSmem);
     cudaFuncSetAttribute(k_spmv_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpmvSmem);
     cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdSmem);
+    cudaFuncSetAttribute(k_update_sr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdSmemSr);
     cudaFuncSetAttribute(k_init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdSmem);
-    int occ_a = 0, occ_b = 0, occ_c = 0;
+    int occ_a = 0, occ_b = 0, occ_c = 0, occ_s = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_spmv_loop, kSpmvThreads, kSpmvSmem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_update, kUpdThreads, kUpdSmem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_pupdate, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k_update_sr, kUpdThreads, kUpdSmemSr);
+    max_grid_sr_ = std::max(1, occ_s) * std::max(1, ctx->sm_count);
     max_grid_a_ = std::max(1, occ_a) * std::max(1, ctx->sm_count);
     max_grid_b_ = std::max(1, occ_b) * std::max(1, ctx->sm_count);
     max_grid_c_ = std::max(1, occ_c) * std::max(1, ctx->sm_count);
@@ -257,6 +261,25 @@ int Engine::push_state(uint32_t s) {
 
 int Engine::add(const MatA *A, const Precond *M, const SolveCfg &cfg, uint32_t *slot_out) {
     if (A->n != M->n) return fail(ctx_, WSB_ERR_BAD_INPUT, "matrix and preconditioner sizes differ (%u vs %u)", A->n, M->n);
+    if (cfg.algorithm != WSB_ALG_CLASSIC && cfg.algorithm != WSB_ALG_SINGLE_REDUCTION)
+        return fail(ctx_, WSB_ERR_BAD_INPUT, "unknown algorithm %d", cfg.algorithm);
+    // One recurrence per engine (its captured loop body is that recurrence's
+    // kernels); an engine with no system left takes the next one's.
+    bool empty = true;
+    for (auto &sl : slots_)
+        if (sl) empty = false;
+    if (empty && algo_ != (uint32_t)cfg.algorithm) {
+        algo_ = (uint32_t)cfg.algorithm;
+        if (exec_) cudaGraphExecDestroy(exec_);
+        if (graph_) cudaGraphDestroy(graph_);
+        exec_ = nullptr;
+        graph_ = nullptr;
+        graph_grid_a_ = graph_grid_b_ = graph_grid_c_ = 0;
+    }
+    if (algo_ != (uint32_t)cfg.algorithm)
+        return fail(ctx_, WSB_ERR_UNSUPPORTED,
+                    "systems iterated together use one recurrence: this batch or server already runs algorithm %u",
+                    algo_);
     uint32_t s = (uint32_t)slots_.size();
     for (uint32_t i = 0; i < slots_.size(); ++i)
         if (!slots_[i]) {
@@ -289,6 +312,7 @@ int Engine::add(const MatA *A, const Precond *M, const SolveCfg &cfg, uint32_t *
     take(8, sizeof(double) * (A->n_stiles + 1));
     take(9, sizeof(double2) * (M->n_utiles + 1));
     take(10, sizeof(double) * (sl->hist_cap + 1));
+    take(11, cfg.algorithm == WSB_ALG_SINGLE_REDUCTION ? vf : 0);  // s
     void *mem = nullptr;
     cudaError_t e = cudaMallocAsync(&mem, tot, stream_);
     if (e != cudaSuccess)
@@ -309,6 +333,7 @@ int Engine::add(const MatA *A, const Precond *M, const SolveCfg &cfg, uint32_t *
     sl->part_a = (double *)(base + off[8]);
     sl->part_b = (double2 *)(base + off[9]);
     sl->hist = sl->hist_cap ? (double *)(base + off[10]) : nullptr;
+    sl->s = cfg.algorithm == WSB_ALG_SINGLE_REDUCTION ? (float *)(base + off[11]) : nullptr;
 
     SysDesc &d = h_sys_[s];
     std::memset(&d, 0, sizeof d);
@@ -340,6 +365,8 @@ int Engine::add(const MatA *A, const Precond *M, const SolveCfg &cfg, uint32_t *
     d.part_b = sl->part_b;
     d.st = d_state_ + s;
     d.history = sl->hist;
+    d.algo = (uint32_t)cfg.algorithm;
+    d.s = sl->s;
     std::memset(h_state_ + s, 0, sizeof(SysState));
     if ((rc = push_desc(s))) return rc;
     if ((rc = push_state(s))) return rc;
@@ -478,8 +505,14 @@ int Engine::capture_loop(uint32_t ga, uint32_t gb, uint32_t gc) {
         const SysDesc *dsys = d_sys_;
         StepParams *dsp = d_sp_;
         cudaError_t le = launch_pdl(k_spmv_loop, ga, kSpmvThreads, kSpmvSmem, cs, dsys, dsp);
-        if (le == cudaSuccess) le = launch_pdl(k_update, gb, kUpdThreads, kUpdSmem, cs, dsys, dsp);
-        if (le == cudaSuccess) le = launch_pdl(k_pupdate, gc, kThreads, (size_t)0, cs, dsys, dsp, h);
+        if (algo_ == WSB_ALG_SINGLE_REDUCTION) {
+            // Two kernels per iteration: the update kernel also forms the new
+            // direction and ends the loop body.
+            if (le == cudaSuccess) le = launch_pdl(k_update_sr, gb, kUpdThreads, kUpdSmemSr, cs, dsys, dsp, h);
+        } else {
+            if (le == cudaSuccess) le = launch_pdl(k_update, gb, kUpdThreads, kUpdSmem, cs, dsys, dsp);
+            if (le == cudaSuccess) le = launch_pdl(k_pupdate, gc, kThreads, (size_t)0, cs, dsys, dsp, h);
+        }
         e = cudaStreamEndCapture(cs, &body);
         if (e == cudaSuccess && le != cudaSuccess) e = le;
     }
@@ -666,7 +699,7 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
     }
     if (num_active_ > 0 && n_work_a_ > 0) {
         const uint32_t ga = std::max<uint32_t>(1, std::min<uint32_t>(n_work_a_, (uint32_t)max_grid_a_));
-        const uint32_t gb = std::max<uint32_t>(1, std::min<uint32_t>(n_work_b_, (uint32_t)max_grid_b_));
+        const uint32_t gb = std::max<uint32_t>(1, std::min<uint32_t>(n_work_b_, (uint32_t)update_grid_max()));
         const uint32_t gc = std::max<uint32_t>(1, std::min<uint32_t>(n_work_c_, (uint32_t)max_grid_c_));
         if (use_graph_) {
             if (!exec_ || ga > graph_grid_a_ || gb > graph_grid_b_ || gc > graph_grid_c_ || 2 * ga < graph_grid_a_ ||
@@ -683,8 +716,12 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
                 const cudaGraphConditionalHandle none = 0;
                 for (uint32_t i = 0; i < burst; ++i) {
                     WSB_CUDA_TRY(ctx_, launch_pdl(k_spmv_loop, ga, kSpmvThreads, kSpmvSmem, stream_, dsys, dsp));
-                    WSB_CUDA_TRY(ctx_, launch_pdl(k_update, gb, kUpdThreads, kUpdSmem, stream_, dsys, dsp));
-                    WSB_CUDA_TRY(ctx_, launch_pdl(k_pupdate, gc, kThreads, (size_t)0, stream_, dsys, dsp, none));
+                    if (algo_ == WSB_ALG_SINGLE_REDUCTION) {
+                        WSB_CUDA_TRY(ctx_, launch_pdl(k_update_sr, gb, kUpdThreads, kUpdSmemSr, stream_, dsys, dsp, none));
+                    } else {
+                        WSB_CUDA_TRY(ctx_, launch_pdl(k_update, gb, kUpdThreads, kUpdSmem, stream_, dsys, dsp));
+                        WSB_CUDA_TRY(ctx_, launch_pdl(k_pupdate, gc, kThreads, (size_t)0, stream_, dsys, dsp, none));
+                    }
                 }
                 WSB_CUDA_TRY(ctx_, cudaGetLastError());
                 done_iters += burst;
@@ -782,7 +819,7 @@ int Engine::profile_kernels(uint32_t s, uint32_t iters, double ms[5]) {
     h_sp_->loop_limit = iters;
     WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_sp_, h_sp_, sizeof(StepParams), cudaMemcpyHostToDevice, stream_));
     const uint32_t ga = std::min<uint32_t>(n_work_a_, (uint32_t)max_grid_a_);
-    const uint32_t gb = std::min<uint32_t>(n_work_b_, (uint32_t)max_grid_b_);
+    const uint32_t gb = std::min<uint32_t>(n_work_b_, (uint32_t)update_grid_max());
     const uint32_t gc = std::min<uint32_t>(n_work_c_, (uint32_t)max_grid_c_);
     k_spmv_init<<<std::min<uint32_t>(h_sp_->n_init_a, (uint32_t)max_grid_a_), kSpmvThreads, kSpmvSmem, stream_>>>(d_sys_, d_sp_);
     k_init<<<std::min<uint32_t>(h_sp_->n_init_b, (uint32_t)max_grid_b_), kUpdThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
@@ -792,9 +829,12 @@ int Engine::profile_kernels(uint32_t s, uint32_t iters, double ms[5]) {
         cudaEventRecord(ev[4 * i + 0], stream_);
         k_spmv_loop<<<ga, kSpmvThreads, kSpmvSmem, stream_>>>(d_sys_, d_sp_);
         cudaEventRecord(ev[4 * i + 1], stream_);
-        k_update<<<gb, kUpdThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
+        if (algo_ == WSB_ALG_SINGLE_REDUCTION)
+            k_update_sr<<<gb, kUpdThreads, kUpdSmemSr, stream_>>>(d_sys_, d_sp_, 0);
+        else
+            k_update<<<gb, kUpdThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
         cudaEventRecord(ev[4 * i + 2], stream_);
-        k_pupdate<<<gc, kThreads, 0, stream_>>>(d_sys_, d_sp_, 0);
+        if (algo_ != WSB_ALG_SINGLE_REDUCTION) k_pupdate<<<gc, kThreads, 0, stream_>>>(d_sys_, d_sp_, 0);
         cudaEventRecord(ev[4 * i + 3], stream_);
     }
     WSB_CUDA_TRY(ctx_, cudaGetLastError());

@@ -85,6 +85,7 @@ struct SolveCfg {
     float inner_rel_tol = 1e-4f;
     uint32_t max_refine = 50;
     uint64_t hist_cap = 0;
+    int algorithm = WSB_ALG_CLASSIC;  // the PCG recurrence (wsb_algorithm)
 };
 
 struct SolveOutcome {
@@ -162,6 +163,9 @@ class Engine {
     cudaGraphExec_t exec_ = nullptr;
     uint32_t graph_grid_a_ = 0, graph_grid_b_ = 0, graph_grid_c_ = 0;
     int max_grid_a_ = 0, max_grid_b_ = 0, max_grid_c_ = 0;
+    int max_grid_sr_ = 0;                   // resident CTAs of k_update_sr
+    uint32_t algo_ = WSB_ALG_CLASSIC;       // the recurrence of every system in this engine
+    int update_grid_max() const { return algo_ == WSB_ALG_SINGLE_REDUCTION ? max_grid_sr_ : max_grid_b_; }
     uint32_t num_active_ = 0;
     double last_device_ms_ = 0.0;
     uint64_t launches_ = 0;

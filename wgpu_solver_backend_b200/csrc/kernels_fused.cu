@@ -312,9 +312,11 @@ struct SpmvDesc {
     const uint32_t *csrc;  // CSR: the staged range's columns, col + ka (read by the gather warp)
 };
 
+// The vector the SpMV multiplies: p (classic loop), u = z (single-reduction
+// loop), x0 (init) or the caller's x (plain).
 template <int kMode>
 __device__ __forceinline__ const float *spmv_input(const SysDesc &S, const float *__restrict__ xplain) {
-    return kMode == M_PLAIN ? xplain : kMode == M_INIT ? S.x : S.p;
+    return kMode == M_PLAIN ? xplain : kMode == M_INIT ? S.x : (S.algo == ALGO_SINGLE_REDUCTION ? S.z : S.p);
 }
 
 // Checks one work index of the SpMV work list (one producer lane): false
@@ -592,9 +594,13 @@ __device__ __forceinline__ float long_tile(const SysDesc &S, const SpmvDesc &d, 
 // most BSR6 tiles and so is free while the others compute.
 constexpr uint32_t kPublisher = NC - 32;
 
-// The last CTA of a system's SpMV tiles: p.Ap from the per-tile partials in
-// tile order, alpha = rz_old / pAp (0 when pAp == 0, as
-// pcg_update_scalars.wgsl:59-62).
+// The last CTA of a system's SpMV tiles. Classic: p.Ap from the per-tile
+// partials in tile order, alpha = rz_old / pAp (0 when pAp == 0, as
+// pcg_update_scalars.wgsl:59-62). Single reduction (the SpMV multiplied u, so
+// the partials sum to delta = (A u, u)), with gamma = (r, u) from the update
+// kernel: beta = gamma / gamma_prev and alpha = gamma / (delta - beta gamma /
+// alpha_prev), or beta = 0 and alpha = gamma / delta in the first iteration;
+// the denominator is kept in pap for the update kernel's breakdown check.
 __device__ __forceinline__ void flush_spmv(const SysDesc *__restrict__ sys, uint32_t s, uint32_t cnt, double *red,
                                            int *s_last) {
     if (cnt == 0) return;
@@ -603,10 +609,25 @@ __device__ __forceinline__ void flush_spmv(const SysDesc *__restrict__ sys, uint
     if (!take_ticket<NC>(&st->cnt_a, cnt, S.n_stiles, s_last, kPublisher)) return;
     const double pap = sum_partials<NC>(S.part_a, S.n_stiles, red);
     if (threadIdx.x == 0) {
-        const double alpha = pap != 0.0 ? st->rz_old / pap : 0.0;
-        st->pap = pap;
-        st->alpha = alpha;
-        st->alpha_f = (float)alpha;
+        if (S.algo == ALGO_SINGLE_REDUCTION) {
+            const double gamma = st->rz_old;
+            double beta = 0.0, den = pap;
+            if (st->iter > 0) {
+                beta = st->gamma_prev != 0.0 ? gamma / st->gamma_prev : 0.0;
+                den = st->alpha != 0.0 ? pap - beta * gamma / st->alpha : 0.0;
+            }
+            const double alpha = den != 0.0 ? gamma / den : 0.0;
+            st->pap = den;
+            st->alpha = alpha;
+            st->alpha_f = (float)alpha;
+            st->beta = beta;
+            st->beta_f = (float)beta;
+        } else {
+            const double alpha = pap != 0.0 ? st->rz_old / pap : 0.0;
+            st->pap = pap;
+            st->alpha = alpha;
+            st->alpha_f = (float)alpha;
+        }
         st->cnt_a = 0;
     }
 }
@@ -829,29 +850,46 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
 // ---------------------------------------------------------------------------
 // Update tiles (x, r, z and the block-Jacobi solve)
 // ---------------------------------------------------------------------------
-constexpr int NU = kUpdConsumers;                         // consumer threads of the update kernels
-constexpr int kVecCap = kUpdTileRows + 8;                 // floats per staged vector slice
-constexpr int kLuOff = 4 * kVecCap;                       // LU blocks
-constexpr int kBsOff = kLuOff + kUpdBlocks * 36;          // block starts slice
-static_assert((kLuOff * 4) % 16 == 0 && (kBsOff * 4) % 16 == 0 && (kVecCap * 4) % 16 == 0, "TMA alignment");
-static_assert(kUpdStageFloats >= kBsOff + kUpdBlocks + 8 && (kUpdStageFloats * 4) % 128 == 0, "stage size");
+// Three kernels share this pipeline (kK):
+//   K_INIT  k_init       r = b + (-1)(A x0); z = M r; p = z; FP64 b.b, r.z
+//   K_LOOP  k_update     x += alpha p; r += (-alpha) Ap; z = M r; FP64 r.r, r.z
+//   K_SR    k_update_sr  single reduction: p = u + beta p; s = w + beta s;
+//                        x += alpha p; r += (-alpha) s; u = M r; FP64 r.r, r.u
+//                        (u lives in z, w = A u in ap)
+// Stage slots (kVecCap floats each): 0 = x (init: b), 1 = p, 2 = r, 3 = Ap
+// (w), and for K_SR 4 = z (u), 5 = s; then the tile's LU blocks and block
+// starts.
+enum UpdKind { K_INIT = 0, K_LOOP = 1, K_SR = 2 };
+constexpr int NU = kUpdConsumers;  // consumer threads of the update kernels
+constexpr int kVecCap = kUpdTileRows + 8;  // floats per staged vector slice
+template <int kK>
+struct UpdLayout {
+    static constexpr int kSlots = kK == K_SR ? 6 : 4;
+    static constexpr int kLuOff = kSlots * kVecCap;          // LU blocks
+    static constexpr int kBsOff = kLuOff + kUpdBlocks * 36;  // block starts slice
+    static constexpr int kStageFloats = kK == K_SR ? kUpdStageFloatsSr : kUpdStageFloats;
+    static_assert((kLuOff * 4) % 16 == 0 && (kBsOff * 4) % 16 == 0 && (kVecCap * 4) % 16 == 0, "TMA alignment");
+    static_assert(kStageFloats >= kBsOff + kUpdBlocks + 8 && (kStageFloats * 4) % 128 == 0, "stage size");
+};
 
 struct UpdDesc {
     uint32_t valid, sys, tile;
     uint32_t row0, rows, blk0, nblk;
     uint32_t ra, ba;  // 4-aligned starts of the staged row / block-start ranges
-    float alpha;      // the system's alpha (loop kernel), read by the producer
-    float *x, *r, *z, *p;
+    float alpha;      // the system's alpha (loop kernels), read by the producer
+    float beta;       // single reduction: the system's beta
+    uint32_t first;   // single reduction: the system's first iteration (p = u, s = w)
+    float *x, *r, *z, *p, *s;
     double2 *part;    // the system's per-tile (r.r, r.z) partials
-    const float *v0, *v1, *v2, *v3;  // bulk-copy sources of the staged vector slots (from ra)
-    const float *lu;                 // bulk-copy source of the tile's LU blocks
-    const uint32_t *bs;              // bulk-copy source of the tile's block starts (from ba)
+    const float *v[6];  // bulk-copy sources of the staged vector slots (from ra)
+    const float *lu;    // bulk-copy source of the tile's LU blocks
+    const uint32_t *bs; // bulk-copy source of the tile's block starts (from ba)
 };
 
 // Checks one work index of the update work list (one producer lane); false
-// past the end, for an invalid item (error code set) and, in the loop kernel,
+// past the end, for an invalid item (error code set) and, in the loop kernels,
 // for a system that is no longer active.
-template <bool kInit>
+template <int kK>
 __device__ __forceinline__ bool check_upd(const SysDesc *__restrict__ sys, const StepParams *sp, uint32_t idx,
                                           uint32_t nw, WorkItem it) {
     if (idx >= nw) return false;
@@ -859,11 +897,11 @@ __device__ __forceinline__ bool check_upd(const SysDesc *__restrict__ sys, const
         atomicOr(const_cast<uint32_t *>(&sp->error), kErrBadItem);  // invalid work item: skipped
         return false;
     }
-    return kInit || sys[it.sys].st->active;
+    return kK == K_INIT || sys[it.sys].st->active;
 }
 
 // Fills the descriptor of a checked work item, field by field, in shared memory.
-template <bool kInit>
+template <int kK>
 __device__ __forceinline__ void fill_upd(const SysDesc *__restrict__ sys, WorkItem it, UpdDesc *d) {
     const SysDesc &S = sys[it.sys];
     const UpdTile T = S.utiles[it.tile];
@@ -877,64 +915,96 @@ __device__ __forceinline__ void fill_upd(const SysDesc *__restrict__ sys, WorkIt
     d->nblk = T.blk1 - T.blk0;
     d->ra = ra;
     d->ba = ba;
-    d->alpha = kInit ? 0.0f : S.st->alpha_f;
+    d->alpha = kK == K_INIT ? 0.0f : S.st->alpha_f;
+    d->beta = kK == K_SR ? S.st->beta_f : 0.0f;
+    d->first = kK == K_SR ? (S.st->iter == 0) : 0u;
     d->x = S.x;
     d->r = S.r;
     d->z = S.z;
     d->p = S.p;
+    d->s = S.s;
     d->part = S.part_b;
-    d->v0 = (kInit ? S.b : S.x) + ra;
-    d->v1 = S.p + ra;
-    d->v2 = S.r + ra;
-    d->v3 = S.ap + ra;
+    d->v[0] = (kK == K_INIT ? S.b : S.x) + ra;
+    d->v[1] = S.p + ra;
+    d->v[2] = S.r + ra;
+    d->v[3] = S.ap + ra;
+    d->v[4] = kK == K_SR ? S.z + ra : nullptr;
+    d->v[5] = kK == K_SR ? S.s + ra : nullptr;
     d->lu = S.lu + (size_t)T.blk0 * 36u;
     d->bs = S.bstart + ba;
 }
 
-// Stage slots: 0 = x (init: b), 1 = p, 2 = r, 3 = Ap; then LU and block starts.
-template <bool kInit>
+template <int kK>
 __device__ __forceinline__ void issue_upd(const UpdDesc &d, float *stage, uint64_t *bar, uint64_t pol) {
+    using Lay = UpdLayout<kK>;
     const uint32_t vc = ((d.row0 + d.rows - d.ra) + 3) & ~3u;
     const uint32_t bc = ((d.blk0 + d.nblk + 1 - d.ba) + 3) & ~3u;
     const uint32_t lub = d.nblk * 144u;
-    const uint32_t nvec = kInit ? 2u : 4u;
+    const uint32_t nvec = kK == K_INIT ? 2u : kK == K_SR ? 6u : 4u;
     mbar_expect_tx(bar, nvec * 4u * vc + lub + 4u * bc);
-    tma_load(stage, d.v0, 4u * vc, bar);
-    if (!kInit) {
-        tma_load(stage + kVecCap, d.v1, 4u * vc, bar);
-        tma_load(stage + 2 * kVecCap, d.v2, 4u * vc, bar);
+    tma_load(stage, d.v[0], 4u * vc, bar);
+    if (kK != K_INIT) {
+        tma_load(stage + kVecCap, d.v[1], 4u * vc, bar);
+        tma_load(stage + 2 * kVecCap, d.v[2], 4u * vc, bar);
     }
-    tma_load(stage + 3 * kVecCap, d.v3, 4u * vc, bar);
-    if (lub) tma_load_stream(stage + kLuOff, d.lu, lub, bar, pol);
-    tma_load_stream(stage + kBsOff, d.bs, 4u * bc, bar, pol);
+    tma_load(stage + 3 * kVecCap, d.v[3], 4u * vc, bar);
+    if (kK == K_SR) {
+        tma_load(stage + 4 * kVecCap, d.v[4], 4u * vc, bar);
+        tma_load(stage + 5 * kVecCap, d.v[5], 4u * vc, bar);
+    }
+    if (lub) tma_load_stream(stage + Lay::kLuOff, d.lu, lub, bar, pol);
+    tma_load_stream(stage + Lay::kBsOff, d.bs, 4u * bc, bar, pol);
 }
 
-// The updated residual of row o of the stage (o relative to the staged
-// range): loop r + (-alpha) Ap (axpy_from_scalar_results.wgsl), init b - A x0
-// (the reference's r = b, r += -1 * Ax).
-template <bool kInit>
-__device__ __forceinline__ float staged_r(const float *stage, uint32_t o, float ma) {
-    return kInit ? __fsub_rn(stage[o], stage[3 * kVecCap + o])
-                 : __fadd_rn(stage[2 * kVecCap + o], __fmul_rn(ma, stage[3 * kVecCap + o]));
+// The row update of staged row o before the block solve: the new residual
+// (returned), and in the stage the row's new x (slot 0) and, for K_SR, its
+// new p (slot 1) and s (slot 5); the new r is written by the caller.
+//   K_INIT r = b + (-1)(A x0)          (the reference's r = b, r += -1 * Ax)
+//   K_LOOP r = r + (-alpha) Ap, x = x + alpha p                (axpy*.wgsl)
+//   K_SR   p = p*beta + u, s = s*beta + w (p = u, s = w in the first
+//          iteration), x = x + alpha p, r = r + (-alpha) s
+// Each thread touches only its own rows, after reading them.
+template <int kK>
+__device__ __forceinline__ float row_update(const UpdDesc &d, float *stage, uint32_t o) {
+    if (kK == K_INIT) return __fsub_rn(stage[o], stage[3 * kVecCap + o]);
+    const float a = d.alpha, ma = -a;
+    if (kK == K_LOOP) {
+        const float ri = __fadd_rn(stage[2 * kVecCap + o], __fmul_rn(ma, stage[3 * kVecCap + o]));
+        stage[o] = __fadd_rn(stage[o], __fmul_rn(a, stage[kVecCap + o]));
+        return ri;
+    }
+    const float u = stage[4 * kVecCap + o], w = stage[3 * kVecCap + o];
+    const float pi = d.first ? u : __fadd_rn(__fmul_rn(stage[kVecCap + o], d.beta), u);
+    const float si = d.first ? w : __fadd_rn(__fmul_rn(stage[5 * kVecCap + o], d.beta), w);
+    stage[kVecCap + o] = pi;
+    stage[5 * kVecCap + o] = si;
+    stage[o] = __fadd_rn(stage[o], __fmul_rn(a, pi));
+    return __fadd_rn(stage[2 * kVecCap + o], __fmul_rn(ma, si));
+}
+
+// Stage slot that receives the new z (u): slot 1 for the classic kernels (p
+// is not needed after the row update; the copy-out writes it to z, and to p
+// in k_init), slot 4 for K_SR.
+template <int kK>
+constexpr int z_slot() {
+    return kK == K_SR ? 4 : 1;
 }
 
 // Block solve of one thread: block blk0 + j of the tile, rows [off, off + m)
-// of the stage (m = min(6, block length)). The thread forms the rows' updated
-// residual from the staged slices itself (loop: r + (-alpha) Ap, init:
-// b - A x0), runs z = U^-1 L^-1 r in registers with the reference's operation
-// order (block_jacobi.wgsl: unit-L forward solve lines 93-101, U backward
-// solve dividing by U(i,i) lines 103-122, rows i < m only, lines 79 and
-// 124-126), and writes its rows' new x (loop), r and z back into the stage
-// (slots 0, 2 and 1; each thread touches only its own rows, after reading
-// them). FP64 r.r (init: b.b) and r.z of the rows go to da and rz.
-template <bool kInit>
+// of the stage (m = min(6, block length)). The thread forms its rows' row
+// update (row_update) itself, runs z = U^-1 L^-1 r in registers with the
+// reference's operation order (block_jacobi.wgsl: unit-L forward solve lines
+// 93-101, U backward solve dividing by U(i,i) lines 103-122, rows i < m only,
+// lines 79 and 124-126), and writes its rows' new r and z back into the
+// stage. FP64 r.r (init: b.b) and r.z of the rows go to da and rz.
+template <int kK>
 __device__ __forceinline__ void bj_block(const UpdDesc &d, float *stage, uint32_t j, double &da, double &rz) {
-    const uint32_t *bs = reinterpret_cast<const uint32_t *>(stage + kBsOff);
+    using Lay = UpdLayout<kK>;
+    const uint32_t *bs = reinterpret_cast<const uint32_t *>(stage + Lay::kBsOff);
     const uint32_t off = bs[d.blk0 + j - d.ba], nxt = bs[d.blk0 + j + 1 - d.ba];
     const uint32_t m = min(nxt - off, 6u);
     const uint32_t ro = off - d.ra;
-    const float ma = -d.alpha;
-    const float2 *L2 = reinterpret_cast<const float2 *>(stage + kLuOff + j * 36u);
+    const float2 *L2 = reinterpret_cast<const float2 *>(stage + Lay::kLuOff + j * 36u);
     float L[36];
 #pragma unroll
     for (int q = 0; q < 18; ++q) {
@@ -945,7 +1015,16 @@ __device__ __forceinline__ void bj_block(const UpdDesc &d, float *stage, uint32_
     float rv[6], y[6], xs[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
-        rv[i] = (uint32_t)i < m ? staged_r<kInit>(stage, ro + i, ma) : 0.0f;
+        if ((uint32_t)i < m) {
+            if (kK == K_INIT) {
+                const float bi = stage[ro + i];
+                da += (double)bi * (double)bi;
+            }
+            rv[i] = row_update<kK>(d, stage, ro + i);
+            if (kK != K_INIT) da += (double)rv[i] * (double)rv[i];
+        } else {
+            rv[i] = 0.0f;
+        }
         y[i] = 0.0f;
         xs[i] = 0.0f;
     }
@@ -972,36 +1051,27 @@ __device__ __forceinline__ void bj_block(const UpdDesc &d, float *stage, uint32_
     for (int i = 0; i < 6; ++i) {
         if ((uint32_t)i < m) {
             const uint32_t o = ro + i;
-            if (kInit) {
-                const float bi = stage[o];
-                da += (double)bi * (double)bi;
-            } else {
-                stage[o] = __fadd_rn(stage[o], __fmul_rn(d.alpha, stage[kVecCap + o]));
-                da += (double)rv[i] * (double)rv[i];
-            }
             stage[2 * kVecCap + o] = rv[i];
-            stage[kVecCap + o] = xs[i];
+            stage[z_slot<kK>() * kVecCap + o] = xs[i];
             rz += (double)rv[i] * (double)xs[i];
         }
     }
 }
 
-// A row the block solve leaves alone (position >= 6 in its block): x and r
-// are updated, z keeps its value (read from memory) and enters r.z as it is.
-template <bool kInit>
+// A row the block solve leaves alone (position >= 6 in its block): the row
+// update applies, z (u) keeps its value and enters r.z as it is.
+template <int kK>
 __device__ __forceinline__ void passive_row(const UpdDesc &d, float *stage, uint32_t row, double &da, double &rz) {
     const uint32_t o = row - d.ra;
-    const float ri = staged_r<kInit>(stage, o, -d.alpha);
-    const float zi = d.z[row];
-    if (kInit) {
+    if (kK == K_INIT) {
         const float bi = stage[o];
         da += (double)bi * (double)bi;
-    } else {
-        stage[o] = __fadd_rn(stage[o], __fmul_rn(d.alpha, stage[kVecCap + o]));
-        da += (double)ri * (double)ri;
     }
+    const float ri = row_update<kK>(d, stage, o);
+    if (kK != K_INIT) da += (double)ri * (double)ri;
+    const float zi = kK == K_SR ? stage[4 * kVecCap + o] : d.z[row];
     stage[2 * kVecCap + o] = ri;
-    stage[kVecCap + o] = zi;
+    stage[z_slot<kK>() * kVecCap + o] = zi;
     rz += (double)ri * (double)zi;
 }
 
@@ -1072,14 +1142,16 @@ __device__ __forceinline__ bool group_ticket(uint32_t *counter, uint32_t cnt, ui
     return last;
 }
 
-// The last CTA of a system's update tiles (kInit = false, k_update): r.r and
-// r.z from the per-tile partials in tile order, then the host-side logic of
-// compute.rs:466-488 on the device: breakdown checks (pAp == 0, then
-// rz_old == 0), stop test r.r <= abs^2 or r.r <= rel^2 b.b, iteration limit,
-// beta = rz_new / rz_old, residual history entry. kInit = true (k_init):
-// b.b and rz_old; b.b == 0 finishes the system with 0 iterations and x
-// untouched (compute.rs:252-254), max_iter == 0 finishes it as not converged.
-template <bool kInit, int GT, int BAR>
+// The last CTA of a system's update tiles: the FP64 sums of the per-tile
+// partials in tile order, then the host-side logic of compute.rs:466-488 on
+// the device. K_LOOP: breakdown checks (pAp == 0, then rz_old == 0), stop
+// test r.r <= abs^2 or r.r <= rel^2 b.b, iteration limit, beta = rz_new /
+// rz_old, residual history entry. K_SR: the same checks and stop test (pap
+// holds the SpMV epilogue's alpha denominator); the scalars of the next
+// iteration come from the next SpMV epilogue. K_INIT: b.b and rz_old; b.b ==
+// 0 finishes the system with 0 iterations and x untouched
+// (compute.rs:252-254), max_iter == 0 finishes it as not converged.
+template <int kK, int GT, int BAR>
 __device__ __forceinline__ void flush_upd(const SysDesc *__restrict__ sys, StepParams *sp, uint32_t s, uint32_t cnt,
                                           double *red, int *s_last, uint32_t lt) {
     if (cnt == 0) return;
@@ -1088,7 +1160,7 @@ __device__ __forceinline__ void flush_upd(const SysDesc *__restrict__ sys, StepP
     if (!group_ticket<GT, BAR>(&st->cnt_b, cnt, S.n_utiles, s_last, lt)) return;
     const double2 sum = group_sum_partials2<GT, BAR>(S.part_b, S.n_utiles, red, lt);
     if (lt != 0) return;
-    if (kInit) {
+    if (kK == K_INIT) {
         st->bb = sum.x;
         st->rz_old = sum.y;
         uint32_t status = ST_RUNNING;
@@ -1119,14 +1191,17 @@ __device__ __forceinline__ void flush_upd(const SysDesc *__restrict__ sys, StepP
         } else if (it + 1 >= st->max_iter) {
             status = ST_MAXITER;
         }
-        const double beta = rz_old != 0.0 ? rz_new / rz_old : 0.0;
-        st->beta = beta;
-        st->beta_f = (float)beta;
+        if (kK == K_LOOP) {
+            const double beta = rz_old != 0.0 ? rz_new / rz_old : 0.0;
+            st->beta = beta;
+            st->beta_f = (float)beta;
+        }
         if (status != ST_RUNNING) {
             st->status = status;
             st->active = 0;
             atomicSub(&sp->num_active, 1u);
         } else {
+            if (kK == K_SR) st->gamma_prev = rz_old;
             st->rz_old = rz_new;
         }
     }
@@ -1135,15 +1210,15 @@ __device__ __forceinline__ void flush_upd(const SysDesc *__restrict__ sys, StepP
 
 // Producer warp of the update ring: the same batched resolution and ring
 // discipline as the SpMV producer.
-template <bool kInit>
+template <int kK>
 __device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, StepParams *sp, float *smem,
                                              uint64_t *full, uint64_t *empty, UpdDesc *desc, UpdDesc *bdesc,
                                              long long lim) {
     constexpr uint32_t NS = kUpdStages;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t G = gridDim.x;
-    const uint32_t nw = kInit ? sp->n_init_b : sp->n_work_b;
-    const WorkItem *__restrict__ work = kInit ? sp->init_b : sp->work_b;
+    const uint32_t nw = kK == K_INIT ? sp->n_init_b : sp->n_work_b;
+    const WorkItem *__restrict__ work = kK == K_INIT ? sp->init_b : sp->work_b;
     uint32_t base = blockIdx.x;
     WorkItem it = {0u, 0u};
     if (base + lane * G < nw) it = work[base + lane * G];
@@ -1151,9 +1226,9 @@ __device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, St
     bool err = false;
     const uint64_t pol = l2_evict_first_policy();
     for (;;) {
-        const bool ok = check_upd<kInit>(sys, sp, base + lane * G, nw, it);
+        const bool ok = check_upd<kK>(sys, sp, base + lane * G, nw, it);
         const uint32_t m = __ballot_sync(0xffffffffu, ok);
-        if (ok) fill_upd<kInit>(sys, it, &bdesc[__popc(m & ((1u << lane) - 1u))]);
+        if (ok) fill_upd<kK>(sys, it, &bdesc[__popc(m & ((1u << lane) - 1u))]);
         const uint32_t cnt = __popc(m);
         base += 32u * G;
         const bool more = base < nw;
@@ -1171,7 +1246,7 @@ __device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, St
                 }
                 if (i < cnt) {
                     desc[s] = bdesc[i];
-                    issue_upd<kInit>(desc[s], smem + s * kUpdStageFloats, &full[s], pol);
+                    issue_upd<kK>(desc[s], smem + s * UpdLayout<kK>::kStageFloats, &full[s], pol);
                     issued = k + 1;
                 } else {  // end marker
                     desc[s].valid = 0;
@@ -1189,22 +1264,21 @@ __device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, St
     }
 }
 
-// Consumers of the update kernels. kInit = false (k_update): x += alpha p;
-// r += (-alpha) Ap; z = M^-1 r; FP64 r.r and r.z per tile. kInit = true
-// (k_init, after k_spmv_init): r = b + (-1)(A x0); z = M^-1 r; p = z; FP64
-// b.b and r.z per tile (compute.rs:226-331). Per-system results are formed by
-// flush_upd. A tile holds at most NU blocks: consumer j solves block j of the
-// tile (bj_block; its rows >= 6, if any, are passive rows) and the rows in
-// front of the tile's first block start (continuation rows of a long block)
-// are shared out. The new x, r and z go back into the stage, and after one
-// barrier all consumers copy the tile's rows out with consecutive threads on
-// consecutive rows. Per tile the consumers pass two barriers: the stage wait
-// (which also keeps the next tile's warp partials out of wred until thread 0
-// has published this tile's) and the one before the copy-out.
-template <bool kInit>
+// Consumers of the update kernels (see UpdKind). Per-system results are
+// formed by flush_upd. A tile holds at most NU blocks: consumer j solves
+// block j of the tile (bj_block; its rows >= 6, if any, are passive rows)
+// and the rows in front of the tile's first block start (continuation rows
+// of a long block) are shared out. The new vectors go back into the stage,
+// and after one barrier all consumers copy the tile's rows out with
+// consecutive threads on consecutive rows. Per tile the consumers pass two
+// barriers: the stage wait (which also keeps the next tile's warp partials
+// out of wred until thread 0 has published this tile's) and the one before
+// the copy-out.
+template <int kK>
 __device__ __forceinline__ void upd_consumers(const SysDesc *__restrict__ sys, StepParams *sp, float *smem,
                                               uint64_t *full, uint64_t *empty, const UpdDesc *desc, double *red,
                                               double2 *wred, int *s_last, int *s_ok, long long lim) {
+    using Lay = UpdLayout<kK>;
     constexpr uint32_t NS = kUpdStages;
     constexpr int BAR = 1;
     const uint32_t lt = threadIdx.x;
@@ -1214,46 +1288,51 @@ __device__ __forceinline__ void upd_consumers(const SysDesc *__restrict__ sys, S
         if (lt == 0) s_ok[k & 1u] = mbar_wait(&full[s], par, lim) ? 1 : 0;
         gsync<NU, BAR>();
         if (!s_ok[k & 1u]) {
-            if (lt == 0) atomicOr(&sp->error, kInit ? kErrInitConsumerWait : kErrUpdConsumerWait);
+            if (lt == 0) atomicOr(&sp->error, kK == K_INIT ? kErrInitConsumerWait : kErrUpdConsumerWait);
             return;
         }
         mbar_observe(&full[s], par, lim);
         const UpdDesc &d = desc[s];
         if (!d.valid) break;
         if (d.sys != run_sys) {
-            flush_upd<kInit, NU, BAR>(sys, sp, run_sys, run_cnt, red, s_last, lt);
+            flush_upd<kK, NU, BAR>(sys, sp, run_sys, run_cnt, red, s_last, lt);
             run_sys = d.sys;
             run_cnt = 0;
         }
-        float *stage = smem + s * kUpdStageFloats;
-        double da = 0.0, rz = 0.0;  // loop: r.r and r.z; init: b.b and r.z
-        const uint32_t *bs = reinterpret_cast<const uint32_t *>(stage + kBsOff);
+        float *stage = smem + s * Lay::kStageFloats;
+        double da = 0.0, rz = 0.0;  // loops: r.r and r.z (r.u); init: b.b and r.z
+        const uint32_t *bs = reinterpret_cast<const uint32_t *>(stage + Lay::kBsOff);
         const uint32_t row1 = d.row0 + d.rows;
         // Continuation rows of a long block that started in an earlier tile.
         const uint32_t lead_end = d.nblk ? bs[d.blk0 - d.ba] : row1;
-        for (uint32_t row = d.row0 + lt; row < lead_end; row += NU) passive_row<kInit>(d, stage, row, da, rz);
+        for (uint32_t row = d.row0 + lt; row < lead_end; row += NU) passive_row<kK>(d, stage, row, da, rz);
         if (lt < d.nblk) {
-            bj_block<kInit>(d, stage, lt, da, rz);
+            bj_block<kK>(d, stage, lt, da, rz);
             // The block's rows >= 6 inside this tile.
             const uint32_t off = bs[d.blk0 + lt - d.ba], nxt = bs[d.blk0 + lt + 1 - d.ba];
             const uint32_t end = min(nxt, row1);
-            for (uint32_t row = off + 6u; row < end; ++row) passive_row<kInit>(d, stage, row, da, rz);
+            for (uint32_t row = off + 6u; row < end; ++row) passive_row<kK>(d, stage, row, da, rz);
         }
         da = warp_sum(da);
         rz = warp_sum(rz);
         if ((lt & 31u) == 0) wred[lt >> 5] = make_double2(da, rz);
         gsync<NU, BAR>();
-        // Copy-out: x (loop), r and z (init: p = z) of the tile's rows.
+        // Copy-out of the tile's rows: x (loops), r, z (u), and p (init: p =
+        // z; single reduction: the new p) and s (single reduction).
         {
             const uint32_t o0 = d.row0 - d.ra;
-            float *const xv = d.x, *const rv = d.r, *const zv = d.z, *const pv = d.p;
+            float *const xv = d.x, *const rv = d.r, *const zv = d.z, *const pv = d.p, *const sv = d.s;
             for (uint32_t t = lt; t < d.rows; t += NU) {
                 const uint32_t i = d.row0 + t, o = o0 + t;
-                if (!kInit) xv[i] = stage[o];
+                if (kK != K_INIT) xv[i] = stage[o];
                 rv[i] = stage[2 * kVecCap + o];
-                const float zi = stage[kVecCap + o];
+                const float zi = stage[z_slot<kK>() * kVecCap + o];
                 zv[i] = zi;
-                if (kInit) pv[i] = zi;
+                if (kK == K_INIT) pv[i] = zi;
+                if (kK == K_SR) {
+                    pv[i] = stage[kVecCap + o];
+                    sv[i] = stage[5 * kVecCap + o];
+                }
             }
         }
         if (lt == 0) {
@@ -1271,11 +1350,12 @@ __device__ __forceinline__ void upd_consumers(const SysDesc *__restrict__ sys, S
         mbar_arrive_warp(&empty[s]);
         ++run_cnt;
     }
-    if (run_sys != 0xffffffffu) flush_upd<kInit, NU, BAR>(sys, sp, run_sys, run_cnt, red, s_last, lt);
+    if (run_sys != 0xffffffffu) flush_upd<kK, NU, BAR>(sys, sp, run_sys, run_cnt, red, s_last, lt);
 }
 
-template <bool kInit>
-__device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, StepParams *sp, float *smem) {
+template <int kK>
+__device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, StepParams *sp, float *smem,
+                                             cudaGraphConditionalHandle h = 0) {
     constexpr uint32_t NS = kUpdStages;
     __shared__ __align__(8) uint64_t full[NS], empty[NS];
     __shared__ UpdDesc desc[NS];
@@ -1295,10 +1375,27 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
     pdl_start();
     const long long lim = wait_limit(sp);
     if (tid >= NU) {
-        if (tid < NU + 32) upd_producer<kInit>(sys, sp, smem, full, empty, desc, bdesc, lim);
+        if (tid < NU + 32) upd_producer<kK>(sys, sp, smem, full, empty, desc, bdesc, lim);
         return;
     }
-    upd_consumers<kInit>(sys, sp, smem, full, empty, desc, red, wred, &s_last, s_ok, lim);
+    upd_consumers<kK>(sys, sp, smem, full, empty, desc, red, wred, &s_last, s_ok, lim);
+    if (kK == K_SR) {
+        // The end of the loop body (there is no p-update kernel in this
+        // recurrence): the last CTA to finish counts the pass and ends the
+        // graph's while loop when no system is active, the step's iteration
+        // budget is used, or a kernel reported an error.
+        if (tid == 0) {
+            __threadfence();
+            if (atomicAdd(&sp->tail_ticket, 1u) + 1u == gridDim.x) {
+                __threadfence();
+                sp->tail_ticket = 0;
+                const uint32_t c = sp->loop_count + 1;
+                sp->loop_count = c;
+                if (h != 0 && (sp->num_active == 0 || c >= sp->loop_limit || sp->error != 0))
+                    cudaGraphSetConditional(h, 0);
+            }
+        }
+    }
 }
 
 }  // namespace
@@ -1321,12 +1418,18 @@ __global__ void __launch_bounds__(kSpmvThreads, kSpmvMinCtas) k_spmv_plain(const
 
 __global__ void __launch_bounds__(kUpdThreads, kUpdMinCtas) k_update(const SysDesc *__restrict__ sys, StepParams *sp) {
     extern __shared__ __align__(128) float smem[];
-    upd_pipeline<false>(sys, sp, smem);
+    upd_pipeline<K_LOOP>(sys, sp, smem);
+}
+
+__global__ void __launch_bounds__(kUpdThreads, kUpdMinCtas) k_update_sr(const SysDesc *__restrict__ sys, StepParams *sp,
+                                                                         cudaGraphConditionalHandle h) {
+    extern __shared__ __align__(128) float smem[];
+    upd_pipeline<K_SR>(sys, sp, smem, h);
 }
 
 __global__ void __launch_bounds__(kUpdThreads, kUpdMinCtas) k_init(const SysDesc *__restrict__ sys, StepParams *sp) {
     extern __shared__ __align__(128) float smem[];
-    upd_pipeline<true>(sys, sp, smem);
+    upd_pipeline<K_INIT>(sys, sp, smem);
 }
 
 // ---------------------------------------------------------------------------
@@ -1348,7 +1451,7 @@ __global__ void __launch_bounds__(kThreads) k_pupdate(const SysDesc *__restrict_
         }
         const SysDesc &S = sys[it.sys];
         const SysState *st = S.st;
-        if (!st->active) continue;
+        if (!st->active || S.algo != ALGO_CLASSIC) continue;
         const float bf = st->beta_f;
         const uint32_t r0 = it.tile * (uint32_t)kChunkRows;
         const uint32_t r1 = min(S.n, r0 + (uint32_t)kChunkRows);

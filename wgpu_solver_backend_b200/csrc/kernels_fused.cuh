@@ -29,6 +29,8 @@ constexpr int kSpmvCsrEnd = 2 * (kCsrCap + 8);
 constexpr int kSpmvRpOff = (((kSpmvCsrEnd > kSpmvBsrEnd) ? kSpmvCsrEnd : kSpmvBsrEnd) + 3) & ~3;
 constexpr int kSpmvStageFloats = ((kSpmvRpOff + kSpmvTileRows + 8) + 31) & ~31;
 constexpr int kUpdStageFloats = ((4 * (kUpdTileRows + 8) + kUpdBlocks * 36 + kUpdBlocks + 8) + 31) & ~31;
+// The single-reduction update kernel stages six vector slices.
+constexpr int kUpdStageFloatsSr = ((6 * (kUpdTileRows + 8) + kUpdBlocks * 36 + kUpdBlocks + 8) + 31) & ~31;
 // Threads per CTA of the TMA-pipelined kernels: consumers (kUpdConsumers in
 // the update kernels, kSpmvConsumers in the SpMV) plus one producer warp,
 // plus the gather warps in the SpMV.
@@ -49,11 +51,14 @@ constexpr int kSpmvThreads = kSpmvConsumers + 32 + 32 * kGatherWarps;
 constexpr int kSpmvMinCtas = WSB_SPMV_MIN_CTAS;
 constexpr size_t kSpmvSmem = (size_t)kSpmvStages * kSpmvStageFloats * sizeof(float);
 constexpr size_t kUpdSmem = (size_t)kUpdStages * kUpdStageFloats * sizeof(float);
+constexpr size_t kUpdSmemSr = (size_t)kUpdStages * kUpdStageFloatsSr * sizeof(float);
 
 // k_spmv_loop: Ap = A p with p.Ap and alpha; k_spmv_init: Ap = A x.
 __global__ void k_spmv_loop(const SysDesc *__restrict__ sys, StepParams *sp);
 __global__ void k_spmv_init(const SysDesc *__restrict__ sys, StepParams *sp);
 __global__ void k_update(const SysDesc *__restrict__ sys, StepParams *sp);
+// Single-reduction recurrence: the update kernel ends the loop body itself.
+__global__ void k_update_sr(const SysDesc *__restrict__ sys, StepParams *sp, cudaGraphConditionalHandle h);
 __global__ void k_init(const SysDesc *__restrict__ sys, StepParams *sp);
 __global__ void k_pupdate(const SysDesc *__restrict__ sys, StepParams *sp, cudaGraphConditionalHandle h);
 __global__ void k_loop_gate(StepParams *sp, cudaGraphConditionalHandle h);

@@ -64,6 +64,7 @@ uint64_t estimate_bytes(const Request &r) {
     uint64_t m = 144 * nb + 4 * (nb + 1) + 16 * (n / 16 + 64) + 1024;            // LU, starts, tiles
     uint64_t v = 6 * 4 * (n + kPadElems) + 8 * (n / 16 + 64) + 16 * (n / 16 + 64) + 8 * 4096;
     if (r.cfg.precision == WSB_PREC_MIXED_F64_IR) v += 12 * (n + kPadElems);
+    if (r.cfg.algorithm == WSB_ALG_SINGLE_REDUCTION) v += 4 * (n + kPadElems);
     v += 8 * std::min<uint64_t>(r.cfg.hist_cap, r.cfg.max_iter + 1);
     return a + m + v;
 }
@@ -353,6 +354,7 @@ extern "C" int wsb_server_submit(wsb_server *s, uint32_t n, const uint32_t *row_
         if (o->inner_rel_tol > 0) c.inner_rel_tol = o->inner_rel_tol;
         if (o->max_refine > 0) c.max_refine = o->max_refine;
         c.hist_cap = o->history_capacity;
+        c.algorithm = o->algorithm;
         r->always_x = o->always_write_x != 0;
         r->x64_out = o->x64_out;
     }

@@ -64,6 +64,12 @@ enum SysStatus : uint32_t {
 
 enum Layout : uint32_t { LAYOUT_CSR = 1, LAYOUT_BSR6 = 2 };
 
+// The PCG recurrence of a system (WSB_ALG_*): the reference's classic one, or
+// the single-reduction recurrence of Chronopoulos and Gear, whose SpMV
+// multiplies u = M r (w = A u) and keeps s = A p by recurrence, so that the
+// direction update p = u + beta p moves into the update kernel.
+enum Algo : uint32_t { ALGO_CLASSIC = 0, ALGO_SINGLE_REDUCTION = 1 };
+
 // Row tile of the SpMV: rows [row0, row1) (CSR) or block rows (BSR6), and
 // their nonzero (or 6x6 block) range [k0, k1). A tile holds at most
 // kCsrCap nonzeros (kBsrCapBlocks blocks) unless it is a single longer row.
@@ -91,6 +97,7 @@ struct alignas(64) SysState {
     uint32_t pad0;
     double rr64, bb64;          // FP64 true residual and ||b||^2 (mixed precision)
     uint32_t cnt_c, pad1;
+    double gamma_prev;          // single reduction: (r, u) of the previous iteration
 };
 
 // Read-mostly description of one system in device memory.
@@ -113,6 +120,8 @@ struct SysDesc {
     double2 *part_b;                   // n_utiles partial pairs
     SysState *st;
     double *history;                   // hist_cap entries or null
+    uint32_t algo, pad_algo;           // Algo
+    float *s;                          // single reduction: s = A p (by recurrence)
 };
 
 // Bits of StepParams::error. The wait bits mean a bounded mbarrier wait ran
@@ -147,7 +156,7 @@ struct StepParams {
     uint32_t loop_limit;               // stop the while loop after this many
     uint32_t error;                    // nonzero: a bounded wait ran out or a work item was invalid
     uint32_t num_sys;                  // entries of the SysDesc array (work items are checked against it)
-    uint32_t pad;
+    uint32_t tail_ticket;              // single reduction: CTAs of the update kernel done (last one ends the step)
     unsigned long long wait_cycles;    // limit of one pipeline wait in SM clock cycles; 0: the default (~2 s)
 };
 
