@@ -466,6 +466,27 @@ def measure_c2(ctx, stream, peak):
                      "iteration_us": ms * 1e3 / it, "iteration_bytes": int(ib),
                      "iteration_gbs": ib * it / (ms / 1e3) / 1e9, "iteration_frac": ib * it / (ms / 1e3) / 1e9 / peak,
                      "matrix_bytes": int(info["device_bytes"])}
+        # The opt-in single-reduction recurrence on the same matrix: two
+        # kernels per iteration, SpMV + 68 n bytes (the update kernel also
+        # reads and writes s and forms p = u + beta p).
+        sr = dict(kw, algorithm=wsb.ALG_SINGLE_REDUCTION)
+        d_x.zero_()
+        m.solve_device(d_b.data_ptr(), d_x.data_ptr(), **sr)  # warm-up
+        ms_sr = 0.0
+        for _ in range(reps):
+            d_x.zero_()
+            torch.cuda.synchronize()
+            e0.record(stream)
+            r_sr = m.solve_device(d_b.data_ptr(), d_x.data_ptr(), **sr)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms_sr += e0.elapsed_time(e1) / reps
+        it_sr = int(r_sr["iterations"])
+        ib_sr = info["spmv_bytes"] + 68 * n
+        out[name + "_single_reduction"] = {"solve_ms": ms_sr, "iterations": it_sr, "iteration_us": ms_sr * 1e3 / it_sr,
+                                           "iteration_bytes": int(ib_sr),
+                                           "iteration_gbs": ib_sr * it_sr / (ms_sr / 1e3) / 1e9,
+                                           "iteration_frac": ib_sr * it_sr / (ms_sr / 1e3) / 1e9 / peak}
         del m
     return out
 
