@@ -31,10 +31,16 @@ int fail(Context *ctx, int status, const char *f, ...) {
     return status;
 }
 
+cudaMemPool_t &thread_alloc_pool() {
+    static thread_local cudaMemPool_t pool = nullptr;
+    return pool;
+}
+
 int dev_alloc(Context *ctx, void **p, size_t bytes, bool zero, cudaStream_t stream) {
     *p = nullptr;
     if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMalloc(p, bytes);
+    cudaMemPool_t pool = thread_alloc_pool();
+    cudaError_t e = pool ? cudaMallocFromPoolAsync(p, bytes, pool, stream) : cudaMalloc(p, bytes);
     if (e != cudaSuccess) {
         *p = nullptr;
         return fail(ctx, e == cudaErrorMemoryAllocation ? WSB_ERR_OUT_OF_MEMORY : WSB_ERR_CUDA,

@@ -31,20 +31,20 @@ static cudaError_t launch_pdl(void (*kernel)(Params...), uint32_t grid, uint32_t
     return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
+static void release(void *p, bool pooled, cudaStream_t st) {
+    if (!p) return;
+    if (pooled) cudaFreeAsync(p, st);
+    else dev_free(p);
+}
+
 MatA::~MatA() {
-    dev_free(row_ptr);
-    dev_free(col);
-    dev_free(val);
-    dev_free(brow_ptr);
-    dev_free(bcol);
-    dev_free(bval);
-    dev_free(stiles);
+    for (void *p : {(void *)row_ptr, (void *)col, (void *)val, (void *)brow_ptr, (void *)bcol, (void *)bval,
+                    (void *)stiles})
+        release(p, pooled, free_stream);
 }
 
 Precond::~Precond() {
-    dev_free(lu);
-    dev_free(bs);
-    dev_free(utiles);
+    for (void *p : {(void *)lu, (void *)bs, (void *)utiles}) release(p, pooled, free_stream);
 }
 
 template <class T>

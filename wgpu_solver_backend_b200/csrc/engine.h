@@ -26,6 +26,10 @@ struct MatA {
     // or brow_ptr for BSR6) and the caps the current tiles were built with.
     std::vector<uint32_t> h_rows;
     uint32_t tile_rows = 0, tile_cap = 0;
+    // Memory drawn from a stream-ordered pool (thread_alloc_pool): released
+    // with cudaFreeAsync on free_stream, which must order after its last use.
+    bool pooled = false;
+    cudaStream_t free_stream = nullptr;
     ~MatA();
 };
 
@@ -41,6 +45,8 @@ struct Precond {
     uint64_t bytes = 0;
     std::vector<uint32_t> h_bs;                 // host copy of the block starts
     uint32_t tile_rows = 0, tile_blocks = 0;    // caps of the current update tiles
+    bool pooled = false;                        // as MatA::pooled
+    cudaStream_t free_stream = nullptr;
     ~Precond();
 };
 

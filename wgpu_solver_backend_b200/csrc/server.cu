@@ -76,6 +76,11 @@ struct wsb_server {
     wsb_server_opts opts{};
     cudaStream_t stream = nullptr;
     std::vector<cudaStream_t> upload_streams;
+    // Device memory of the requests' matrices and factors: a stream-ordered
+    // pool that keeps up to the budget cached, so that admitting and retiring
+    // requests never calls cudaMalloc/cudaFree (a cudaFree waits for all work
+    // in flight on the GPU, the uploads of other requests included).
+    cudaMemPool_t pool = nullptr;
     std::unique_ptr<Engine> eng;
     std::mutex mu;
     std::condition_variable cv_upload, cv_sched, cv_done;
@@ -113,6 +118,7 @@ struct wsb_server {
 
     void upload_loop(cudaStream_t upload_stream) {
         cudaSetDevice(ctx->device);
+        thread_alloc_pool() = pool;
         for (;;) {
             Request *r = nullptr;
             {
@@ -146,8 +152,7 @@ struct wsb_server {
             if (opts.flags & WSB_SERVER_DEVICE_PREP) {
                 // O(n) checks and the tile lists on the host; the column
                 // check, the BSR6 conversion and the LU on the GPU.
-                r->A.reset(new MatA());
-                r->M.reset(new Precond());
+                new_parts(r, upload_stream);
                 rc = prepare_system_device(ctx, r->n, r->p_row_ptr, r->p_col, r->p_val, r->nnz, r->p_bs, r->bs_len,
                                            WSB_LAYOUT_AUTO, upload_stream, r->A.get(), r->M.get());
                 if (rc) err = thread_error();
@@ -161,8 +166,7 @@ struct wsb_server {
                 }
                 prep_ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
                 if (!rc) {
-                    r->A.reset(new MatA());
-                    r->M.reset(new Precond());
+                    new_parts(r, upload_stream);
                     rc = upload_matA(ctx, r->n, r->p_row_ptr, r->p_col, r->p_val, r->nnz, r->p_bs, r->bs_len,
                                      WSB_LAYOUT_AUTO, upload_stream, r->A.get());
                     if (!rc) rc = upload_precond(ctx, r->n, lu.data(), r->p_bs, r->bs_len, upload_stream, r->M.get());
@@ -183,10 +187,22 @@ struct wsb_server {
                 cv_upload.notify_all();
                 continue;
             }
+            // From here on the scheduler's stream orders the release.
+            r->A->free_stream = stream;
+            r->M->free_stream = stream;
             r->state = Request::READY;
             ready.push_back(r);
             cv_sched.notify_all();
         }
+    }
+
+    // The request's matrix and factor objects; their memory comes from the
+    // pool and is released on the upload stream until the request is ready.
+    void new_parts(Request *r, cudaStream_t upload_stream) {
+        r->A.reset(new MatA());
+        r->M.reset(new Precond());
+        r->A->pooled = r->M->pooled = pool != nullptr;
+        r->A->free_stream = r->M->free_stream = upload_stream;
     }
 
     void sched_loop() {
@@ -297,6 +313,16 @@ extern "C" int wsb_server_create(wsb_context *ctx_in, const wsb_server_opts *opt
         return fail(ctx, WSB_ERR_CUDA, "server stream creation failed: %s", cudaGetErrorString(e));
     }
     s->eng.reset(new Engine(ctx, s->stream));
+    cudaMemPoolProps pp = {};
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = ctx->device;
+    if (cudaMemPoolCreate(&s->pool, &pp) == cudaSuccess) {
+        uint64_t keep = s->opts.memory_budget_bytes;
+        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    } else {
+        s->pool = nullptr;  // plain cudaMalloc/cudaFree then
+    }
     // Several uploaders: host preparation of one large request (validation,
     // LU, BSR6 conversion, copies) overlaps with that of the next ones.
     const unsigned n_up = std::max(1u, std::min(4u, std::thread::hardware_concurrency() / 2));
@@ -441,6 +467,9 @@ extern "C" void wsb_server_destroy(wsb_server *s) {
     cudaSetDevice(s->ctx->device);
     s->eng.reset();
     s->table.clear();
+    cudaStreamSynchronize(s->stream);
+    for (cudaStream_t us : s->upload_streams) cudaStreamSynchronize(us);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
     cudaStreamDestroy(s->stream);
     for (cudaStream_t us : s->upload_streams) cudaStreamDestroy(us);
     delete s;

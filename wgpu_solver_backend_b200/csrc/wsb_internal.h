@@ -205,6 +205,12 @@ struct Buffer {
 // non-blocking streams).
 int dev_alloc(Context *ctx, void **p, size_t bytes, bool zero, cudaStream_t stream);
 void dev_free(void *p);
+// A memory pool that dev_alloc draws from on the calling thread (stream
+// ordered, cudaMallocFromPoolAsync on the given stream) instead of
+// cudaMalloc, or null. The server's uploader threads set it, so that
+// retiring a request frees its matrix with cudaFreeAsync instead of a
+// cudaFree, which would wait for every copy and kernel in flight on the GPU.
+cudaMemPool_t &thread_alloc_pool();
 
 // ---------------------------------------------------------------------------
 // Host-side setup helpers (host_setup.cpp)
