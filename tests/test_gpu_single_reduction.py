@@ -6,7 +6,7 @@ update kernel and an iteration is two fused kernels instead of three. The
 checks: it agrees with the oracle's statement of the same recurrence
 (orc_pcg_single_reduction_f64dot: same iteration count within 1, solution
 within 1e-5 relative), with the classic product path (iterations within 2 %,
-solution within 1e-5 relative), passes the datasets' compare-x gates, gives
+distance to the FP64 solution at most twice the classic one's), passes the datasets' compare-x gates, gives
 each system the same bits alone and batched, and carries FP64 refinement to a
 true relative residual of 1e-10.
 """
@@ -41,7 +41,12 @@ def test_single_reduction_matches_its_oracle_and_the_classic_path(ctx, side, ani
     assert abs(int(r["iterations"]) - int(o["iterations"])) <= 1, (r["iterations"], o["iterations"])
     assert rel(x, o["x"]) <= 1e-5, rel(x, o["x"])
     assert abs(int(r["iterations"]) - int(rc["iterations"])) <= max(1, 0.02 * int(rc["iterations"]))
-    assert rel(x, xc) <= 1e-5, rel(x, xc)
+    # Two recurrences stopped at the same recursive residual differ by about
+    # their own solution errors: the bar against the classic path is that
+    # the single-reduction solution is no further from the FP64 solution than
+    # twice the classic one (or 1e-5).
+    x64 = oracle.pcg_f64(s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], s["b"], rel_tol=1e-13)["x"]
+    assert rel(x, x64) <= max(1e-5, 2.0 * rel(xc, x64)), (rel(x, x64), rel(xc, x64))
 
 
 @pytest.mark.parametrize("k", [1, 2, 3])

@@ -35,18 +35,18 @@ constexpr int kUpdStageFloatsSr = ((6 * (kUpdTileRows + 8) + kUpdBlocks * 36 + k
 // the update kernels, kSpmvConsumers in the SpMV) plus one producer warp,
 // plus the gather warps in the SpMV.
 #ifndef WSB_GATHER_WARPS
-#define WSB_GATHER_WARPS 1
+#define WSB_GATHER_WARPS 2
 #endif
 constexpr int kGatherWarps = WSB_GATHER_WARPS;
 constexpr int kUpdThreads = kUpdConsumers + 32;
 #ifndef WSB_UPD_MIN_CTAS
-#define WSB_UPD_MIN_CTAS 3
+#define WSB_UPD_MIN_CTAS 2
 #endif
 constexpr int kUpdMinCtas = WSB_UPD_MIN_CTAS;
 constexpr int kSpmvThreads = kSpmvConsumers + 32 + 32 * kGatherWarps;
 // CTAs per SM the SpMV kernels are compiled for (register budget).
 #ifndef WSB_SPMV_MIN_CTAS
-#define WSB_SPMV_MIN_CTAS 4
+#define WSB_SPMV_MIN_CTAS 3
 #endif
 constexpr int kSpmvMinCtas = WSB_SPMV_MIN_CTAS;
 constexpr size_t kSpmvSmem = (size_t)kSpmvStages * kSpmvStageFloats * sizeof(float);

@@ -29,16 +29,16 @@ namespace wsb {
 #define WSB_BSR_CAP 128
 #endif
 #ifndef WSB_SPMV_STAGES
-#define WSB_SPMV_STAGES 2
+#define WSB_SPMV_STAGES 3
 #endif
 #ifndef WSB_UPD_STAGES
-#define WSB_UPD_STAGES 4
+#define WSB_UPD_STAGES 3
 #endif
 #ifndef WSB_SPMV_CONSUMERS
 #define WSB_SPMV_CONSUMERS 128
 #endif
 #ifndef WSB_UPD_CONSUMERS
-#define WSB_UPD_CONSUMERS 64
+#define WSB_UPD_CONSUMERS 128
 #endif
 constexpr int kThreads = 256;        // threads per CTA of the vector and refinement kernels
 constexpr int kUpdConsumers = WSB_UPD_CONSUMERS;   // consumer threads per CTA of the update kernels
