@@ -302,7 +302,7 @@ SERVER_VARIANTS = {"copy+host_prep": dict(borrow_inputs=False, device_prep=False
                    "borrow+host_prep": dict(borrow_inputs=True, device_prep=False),
                    "copy+device_prep": dict(borrow_inputs=False, device_prep=True),
                    "borrow+device_prep": dict(borrow_inputs=True, device_prep=True)}
-SERVER_CFG = SERVER_VARIANTS["borrow+host_prep"]
+SERVER_CFG = SERVER_VARIANTS["borrow+device_prep"]
 
 
 def mixed_kw():
@@ -535,6 +535,23 @@ def measure_c4(ctx, stream, peak):
             "algorithmic_bytes": int(byts), "gbs": byts / t / 1e9, "frac": byts / t / 1e9 / peak}
 
 
+def pinned_system(sysm):
+    """The system's host arrays moved into page-locked (pinned) host memory,
+    where requests come from in the end-to-end figure: host-to-device copies
+    then run at DMA speed instead of through the driver's staging buffers."""
+    import torch
+
+    out = dict(sysm)
+    for k in ("row_ptr", "col_idx", "values", "block_starts", "b"):
+        a = np.ascontiguousarray(sysm[k])
+        t = torch.empty(max(a.nbytes, 1), dtype=torch.uint8, pin_memory=True)
+        v = t.numpy()[: a.nbytes].view(a.dtype)
+        v[...] = a
+        out[k] = v
+        out["_pin_" + k] = t  # keeps the pinned buffer alive
+    return out
+
+
 def run_serve(args, world, rank, local):
     import torch
 
@@ -549,7 +566,7 @@ def run_serve(args, world, rank, local):
     t_gen = time.perf_counter()
     pool = []
     for side, seed in reqs:
-        sysm = serve_system(side, seed)
+        sysm = pinned_system(serve_system(side, seed))
         sysm["side"], sysm["seed"] = side, seed
         pool.append(sysm)
     t_gen = time.perf_counter() - t_gen
