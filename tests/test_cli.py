@@ -300,3 +300,26 @@ def test_run_pcg_case_failure_is_reported_in_metrics(tmp_path):
     assert m["solver"]["final_relres_true_f64"] is None and m["solver"]["gbps"] is None
     assert not out_x.exists()
     assert r.stderr.startswith("Solve failed: ")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k", [2, 3])
+def test_run_pcg_case_single_reduction(tmp_path, k):
+    """--algorithm single-reduction: the opt-in recurrence through the CLI
+    passes the dataset's compare-x gate, and the metrics name it and count
+    its extra vector (4 bytes per row more than the classic iteration)."""
+    case, _, fx = load_case(k)
+    out_x, out_m = tmp_path / "out" / "x.bin", tmp_path / "out" / "metrics.json"
+    r = run(CLI, "run-pcg-case", "--case-dir", os.path.join(GOLDEN, f"case_{k}"), "--max-iters", "2000",
+            "--rel-tol", "1e-4", "--abs-tol", "1e-7", "--out-x", out_x, "--out-metrics", out_m,
+            "--algorithm", "single-reduction")
+    assert r.returncode == 0, r.stderr
+    m = json.loads(out_m.read_text())
+    assert m["converged"] is True and m["solver"]["algorithm"] == "single-reduction"
+    n, nnz, nb = case.a.n_rows, case.a.nnz, len(case.block_starts) - 1
+    assert m["solver"]["iteration_bytes"] == 8 * nnz + 4 * (n + 1) + 52 * n + 144 * nb
+    assert abs(m["iterations"] - int(fx["iterations"])) <= max(2, 0.02 * int(fx["iterations"]))
+    rel, atol = COMPARE_X_GATES[k]
+    c = run(CLI, "compare-x", "--x-ref", os.path.join(GOLDEN, f"case_{k}", "x_ref.bin"), "--x", out_x,
+            "--rel-tol", str(rel), "--abs-tol", str(atol))
+    assert c.returncode == 0, c.stdout + c.stderr

@@ -64,6 +64,7 @@ void print_help() {
         "run-pcg-case: --case-dir DIR --out-x PATH --out-metrics PATH [--max-iters 2000]\n"
         "              [--rel-tol 1e-8] [--abs-tol 0] [--precision f32-f64dot|reference-f32|mixed]\n"
         "              [--target-relres 1e-10] [--layout executors|auto|csr|bsr6] [--out-history PATH]\n"
+        "              [--algorithm classic|single-reduction]\n"
         "              [--hbm-peak-gbs 7700]\n"
         "compare-x:    --x-ref PATH --x PATH [--rel-tol 1e-3] [--abs-tol 1e-4] [--top-k 10]\n");
 }
@@ -335,6 +336,13 @@ int parse_precision(const Args &a) {
     usage_error("invalid value '" + p + "' for '--precision' [possible values: f32-f64dot, reference-f32, mixed]");
 }
 
+int parse_algorithm(const Args &a) {
+    const std::string p = get(a, "algorithm", "classic");
+    if (p == "classic") return WSB_ALG_CLASSIC;
+    if (p == "single-reduction") return WSB_ALG_SINGLE_REDUCTION;
+    usage_error("invalid value '" + p + "' for '--algorithm' [possible values: classic, single-reduction]");
+}
+
 struct SolveOut {
     uint64_t iterations = 0;
     std::vector<float> x;
@@ -360,6 +368,7 @@ std::string run_pcg_case(wsb_context *ctx, const Args &a, uint64_t max_iters, fl
     wsb_solve_opts opts;
     wsb_solve_opts_default(&opts);
     opts.precision = parse_precision(a);
+    opts.algorithm = parse_algorithm(a);
     opts.target_relres = atof(get(a, "target-relres", "1e-10").c_str());
     const bool want_hist = a.kv.count("out-history");
     if (want_hist) {
@@ -415,6 +424,8 @@ std::string run_pcg_case(wsb_context *ctx, const Args &a, uint64_t max_iters, fl
         wsb_matrix_destroy(m);
     }
     if (!e.empty()) return e;
+    // The single-reduction iteration also reads and writes s = A p.
+    if (opts.algorithm == WSB_ALG_SINGLE_REDUCTION) o->iteration_bytes += 4ull * n;
     o->n = n;
     o->nnz = c.a.nnz;
     if (want_hist) o->history.resize(o->res.history_len);
@@ -433,6 +444,7 @@ int cmd_run_pcg_case(const Args &a) {
     const float rel = strtof(get(a, "rel-tol", "1e-8").c_str(), nullptr);
     const float abs_tol = strtof(get(a, "abs-tol", "0").c_str(), nullptr);
     parse_precision(a);  // usage errors before any work
+    parse_algorithm(a);
     const auto t0 = Clock::now();
     const auto t_gpu0 = Clock::now();
     wsb_context *ctx = context_or_exit(a.device);
@@ -498,6 +510,7 @@ int cmd_run_pcg_case(const Args &a) {
     // Fields of this implementation only; the reference's keys come first.
     j.obj("solver");
     j.raw("precision", json_str(precision_name(parse_precision(a))));
+    j.raw("algorithm", json_str(get(a, "algorithm", "classic")));
     j.raw("path", json_str(get(a, "layout", "executors")));
     j.raw("device_ms", json_f64(o.res.device_ms));
     j.raw("final_r_norm2", json_f64(o.res.final_r_norm2));
