@@ -389,13 +389,14 @@ __device__ __forceinline__ void issue_spmv(const SpmvDesc &d, float *stage, uint
 // into xg[j - ka] by 4-byte cp.async. The columns are read here with
 // streaming 16-byte loads (8 in flight per lane) and never staged; indices
 // outside [k0, k1) belong to neighbouring tiles or the zero padding of the
-// column array, so every gathered address is a valid row of x.
+// column array, so every gathered address is a valid row of x. Each lane
+// keeps WSB_CSR_GATHER_BATCH column loads in flight per round.
 __device__ __forceinline__ void gather_csr(const SpmvDesc &d, float *stage, uint32_t lane) {
     const float *__restrict__ xin = d.x;
     float *xg = stage + kColOff;
     const uint4 *__restrict__ c4 = reinterpret_cast<const uint4 *>(d.csrc);
     const uint32_t nq = (((d.k1 - d.ka) + 3) & ~3u) >> 2;  // 16-byte groups of columns
-    constexpr uint32_t kBatch = 8;
+    constexpr uint32_t kBatch = WSB_CSR_GATHER_BATCH;
     for (uint32_t q0 = 0; q0 < nq; q0 += 32u * kBatch) {
         uint4 c[kBatch];
 #pragma unroll

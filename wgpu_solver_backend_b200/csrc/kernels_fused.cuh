@@ -38,6 +38,10 @@ constexpr int kUpdStageFloatsSr = ((6 * (kUpdTileRows + 8) + kUpdBlocks * 36 + k
 #define WSB_GATHER_WARPS 2
 #endif
 constexpr int kGatherWarps = WSB_GATHER_WARPS;
+// 16-byte column loads each gather lane keeps in flight for a CSR tile.
+#ifndef WSB_CSR_GATHER_BATCH
+#define WSB_CSR_GATHER_BATCH 8
+#endif
 // WSB_UPDATE_DIRECT=1 builds the update kernels without shared-memory
 // staging (each thread loads its block from global memory).
 #ifndef WSB_UPDATE_DIRECT
