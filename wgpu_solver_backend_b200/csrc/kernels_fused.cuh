@@ -50,7 +50,7 @@ constexpr int kGatherWarps = WSB_GATHER_WARPS;
 constexpr bool kUpdDirect = WSB_UPDATE_DIRECT != 0;
 constexpr int kUpdThreads = kUpdDirect ? kUpdConsumers : kUpdConsumers + 32;
 #ifndef WSB_UPD_MIN_CTAS
-#define WSB_UPD_MIN_CTAS 2
+#define WSB_UPD_MIN_CTAS 3
 #endif
 constexpr int kUpdMinCtas = WSB_UPD_MIN_CTAS;
 constexpr int kSpmvThreads = kSpmvConsumers + 32 + 32 * kGatherWarps;

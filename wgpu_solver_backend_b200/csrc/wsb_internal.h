@@ -32,7 +32,7 @@ namespace wsb {
 #define WSB_SPMV_STAGES 3
 #endif
 #ifndef WSB_UPD_STAGES
-#define WSB_UPD_STAGES 3
+#define WSB_UPD_STAGES 2
 #endif
 #ifndef WSB_SPMV_CONSUMERS
 #define WSB_SPMV_CONSUMERS 128
