@@ -302,7 +302,7 @@ SERVER_VARIANTS = {"copy+host_prep": dict(borrow_inputs=False, device_prep=False
                    "borrow+host_prep": dict(borrow_inputs=True, device_prep=False),
                    "copy+device_prep": dict(borrow_inputs=False, device_prep=True),
                    "borrow+device_prep": dict(borrow_inputs=True, device_prep=True)}
-SERVER_CFG = SERVER_VARIANTS["borrow+device_prep"]
+SERVER_CFG = SERVER_VARIANTS["borrow+host_prep"]
 
 
 def mixed_kw():

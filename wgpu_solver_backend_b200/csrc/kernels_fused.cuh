@@ -42,13 +42,7 @@ constexpr int kGatherWarps = WSB_GATHER_WARPS;
 #ifndef WSB_CSR_GATHER_BATCH
 #define WSB_CSR_GATHER_BATCH 8
 #endif
-// WSB_UPDATE_DIRECT=1 builds the update kernels without shared-memory
-// staging (each thread loads its block from global memory).
-#ifndef WSB_UPDATE_DIRECT
-#define WSB_UPDATE_DIRECT 0
-#endif
-constexpr bool kUpdDirect = WSB_UPDATE_DIRECT != 0;
-constexpr int kUpdThreads = kUpdDirect ? kUpdConsumers : kUpdConsumers + 32;
+constexpr int kUpdThreads = kUpdConsumers + 32;
 #ifndef WSB_UPD_MIN_CTAS
 #define WSB_UPD_MIN_CTAS 3
 #endif
@@ -60,8 +54,8 @@ constexpr int kSpmvThreads = kSpmvConsumers + 32 + 32 * kGatherWarps;
 #endif
 constexpr int kSpmvMinCtas = WSB_SPMV_MIN_CTAS;
 constexpr size_t kSpmvSmem = (size_t)kSpmvStages * kSpmvStageFloats * sizeof(float);
-constexpr size_t kUpdSmem = kUpdDirect ? 0 : (size_t)kUpdStages * kUpdStageFloats * sizeof(float);
-constexpr size_t kUpdSmemSr = kUpdDirect ? 0 : (size_t)kUpdStages * kUpdStageFloatsSr * sizeof(float);
+constexpr size_t kUpdSmem = (size_t)kUpdStages * kUpdStageFloats * sizeof(float);
+constexpr size_t kUpdSmemSr = (size_t)kUpdStages * kUpdStageFloatsSr * sizeof(float);
 
 // k_spmv_loop: Ap = A p with p.Ap and alpha; k_spmv_init: Ap = A x.
 __global__ void k_spmv_loop(const SysDesc *__restrict__ sys, StepParams *sp);
