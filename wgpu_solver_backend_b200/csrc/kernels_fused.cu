@@ -73,6 +73,22 @@ __device__ __forceinline__ void tma_load_stream(void *dst, const void *src, uint
         : "memory");
 }
 
+// Read-only 4-byte load of the index data the gather warps read every
+// iteration (row pointers, BSR6 block columns). With WSB_GATHER_KEEP_L2 it
+// carries an L2 evict-last hint: that data is small next to the block values
+// and can stay in the L2 between iterations.
+__device__ __forceinline__ uint32_t ldg_index(const uint32_t *p) {
+#if WSB_GATHER_KEEP_L2
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    uint32_t v;
+    asm volatile("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+#else
+    return __ldg(p);
+#endif
+}
+
 // Asynchronous 4- and 8-byte copies global -> shared (cp.async): the
 // gathered x values go straight into the stage without holding registers.
 __device__ __forceinline__ void cp_async4(void *dst, const void *src) {
@@ -426,7 +442,7 @@ __device__ __forceinline__ void gather_csr(const SpmvDesc &d, float *stage, uint
 // gathers run while the values stream in.
 __device__ __forceinline__ void gather_tile(const SpmvDesc &d, float *stage, uint32_t lane) {
     uint32_t *rp = reinterpret_cast<uint32_t *>(stage + kRpOff);
-    for (uint32_t i = lane; i <= d.nr; i += 32u) rp[i] = __ldg(d.rptr + i);
+    for (uint32_t i = lane; i <= d.nr; i += 32u) rp[i] = ldg_index(d.rptr + i);
     if (d.layout != LAYOUT_BSR6) {
         gather_csr(d, stage, lane);
         return;
@@ -443,7 +459,7 @@ __device__ __forceinline__ void gather_tile(const SpmvDesc &d, float *stage, uin
 #pragma unroll
     for (int q = 0; q < kPer; ++q) {
         const uint32_t blk = lane + 32u * q;
-        c[q] = blk < nb ? __ldg(d.cols + blk) : 0u;
+        c[q] = blk < nb ? ldg_index(d.cols + blk) : 0u;
     }
 #pragma unroll
     for (int q = 0; q < kPer; ++q) {

@@ -38,6 +38,11 @@ constexpr int kUpdStageFloatsSr = ((6 * (kUpdTileRows + 8) + kUpdBlocks * 36 + k
 #define WSB_GATHER_WARPS 2
 #endif
 constexpr int kGatherWarps = WSB_GATHER_WARPS;
+// 1: the gather warps read row pointers and BSR6 block columns with an L2
+// evict-last hint.
+#ifndef WSB_GATHER_KEEP_L2
+#define WSB_GATHER_KEEP_L2 0
+#endif
 // 16-byte column loads each gather lane keeps in flight for a CSR tile.
 #ifndef WSB_CSR_GATHER_BATCH
 #define WSB_CSR_GATHER_BATCH 8
