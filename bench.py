@@ -302,7 +302,7 @@ SERVER_VARIANTS = {"copy+host_prep": dict(borrow_inputs=False, device_prep=False
                    "borrow+host_prep": dict(borrow_inputs=True, device_prep=False),
                    "copy+device_prep": dict(borrow_inputs=False, device_prep=True),
                    "borrow+device_prep": dict(borrow_inputs=True, device_prep=True)}
-SERVER_CFG = SERVER_VARIANTS["borrow+host_prep"]
+SERVER_CFG = SERVER_VARIANTS["borrow+device_prep"]
 
 
 def mixed_kw():
@@ -535,6 +535,17 @@ def measure_c4(ctx, stream, peak):
             "algorithmic_bytes": int(byts), "gbs": byts / t / 1e9, "frac": byts / t / 1e9 / peak}
 
 
+def fcfs_latencies(arrivals_s, service_ms):
+    """Latencies (ms) of requests served one at a time in arrival order, each
+    starting when it has arrived and the previous one has finished."""
+    t, out = 0.0, []
+    for a, sv in zip(arrivals_s, service_ms):
+        start = max(t, float(a))
+        t = start + sv / 1e3
+        out.append((t - float(a)) * 1e3)
+    return out
+
+
 def pinned_system(sysm):
     """The system's host arrays moved into page-locked (pinned) host memory,
     where requests come from in the end-to-end figure: host-to-device copies
@@ -671,6 +682,19 @@ def run_serve(args, world, rank, local):
         m.solve(p["b"], raise_on_error=False, **kw)
     torch.cuda.synchronize()
     plain_res_s = time.perf_counter() - t0
+    # Latency at an arrival rate the plain path can sustain too (70 % of its
+    # own capacity): the served latencies measured on a fresh server, and the
+    # plain path's first-come-first-served latencies for the same arrivals,
+    # replayed from its measured per-request times (one request at a time,
+    # each starting when it has arrived and the previous one is done).
+    lam2 = 0.7 * R / plain_s
+    arrivals2 = np.cumsum(np.random.default_rng(12).exponential(1.0 / lam2, R))
+    srv2 = wsb.Server(ctx, memory_budget_bytes=120 << 30, iters_per_step=16, **SERVER_CFG)
+    served_pass(srv2, pool[: min(8, R)])
+    _, lat_p2, _ = served_pass(srv2, pool, arrivals2)
+    srv2.close()
+    fcfs1 = fcfs_latencies(arrivals, plain_lat)
+    fcfs2 = fcfs_latencies(arrivals2, plain_lat)
     # Dominant kernel (SpMV + p.Ap) on the largest system of the set.
     big = int(np.argmax([p["n"] for p in pool]))
     d_b = torch.from_numpy(pool[big]["b"]).cuda()
@@ -700,7 +724,14 @@ def run_serve(args, world, rank, local):
             for p in pool)), "d2h_bytes_per_step": int(sum(4 * p["n"] for p in pool))},
         "latency_ms": {"p50": float(np.percentile(lat_p, 50)), "p99": float(np.percentile(lat_p, 99)),
                        "arrival_rate_per_s": lam, "burst_p50": float(np.percentile(lats, 50)),
-                       "burst_p99": float(np.percentile(lats, 99))},
+                       "burst_p99": float(np.percentile(lats, 99)),
+                       "plain_fcfs_same_arrivals_p50": float(np.percentile(fcfs1, 50)),
+                       "plain_fcfs_same_arrivals_p99": float(np.percentile(fcfs1, 99)),
+                       "at_plain_sustainable_rate": {
+                           "arrival_rate_per_s": lam2, "served_p50": float(np.percentile(lat_p2, 50)),
+                           "served_p99": float(np.percentile(lat_p2, 99)),
+                           "plain_fcfs_p50": float(np.percentile(fcfs2, 50)),
+                           "plain_fcfs_p99": float(np.percentile(fcfs2, 99))}},
         "plain_sequential": {"solves_per_s": R / plain_s, "resident_solves_per_s": R / plain_res_s,
                              "p50_ms": float(np.percentile(plain_lat, 50)), "p99_ms": float(np.percentile(plain_lat, 99))},
         "speedup_vs_plain": {"e2e": e2e / (world * R / plain_s), "resident": (world * args.steps * R / dev_s) /

@@ -92,3 +92,10 @@ def test_reference_arm_line_on_one_rank():
     # The reference process maps the oracle and never the product library.
     assert d["repo_libraries_loaded"] == ["oracle/liboracle.so"]
     assert d["e2e"] == {"value": d["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_fcfs_replay_of_the_plain_path():
+    # One request at a time in arrival order: a request waits for the one
+    # before it to finish.
+    lat = bench.fcfs_latencies([0.0, 0.1, 0.15, 2.0], [200.0, 50.0, 10.0, 5.0])
+    assert lat == pytest.approx([200.0, 150.0, 110.0, 5.0])

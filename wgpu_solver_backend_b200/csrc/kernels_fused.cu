@@ -73,6 +73,15 @@ __device__ __forceinline__ void tma_load_stream(void *dst, const void *src, uint
         : "memory");
 }
 
+// Bulk prefetch of a global range into the L2 (no completion tracking). The
+// range is widened to 16-byte boundaries; every array it is used on has tail
+// padding, so the widened range stays inside its allocation.
+__device__ __forceinline__ void l2_prefetch(const void *p, uint32_t bytes) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p) & ~uintptr_t(15);
+    const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + bytes + 15) & ~uintptr_t(15);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
+}
+
 // Read-only 4-byte load of the index data the gather warps read every
 // iteration (row pointers, BSR6 block columns). With WSB_GATHER_KEEP_L2 it
 // carries an L2 evict-last hint: that data is small next to the block values
@@ -651,6 +660,17 @@ __device__ __forceinline__ void flush_spmv(const SysDesc *__restrict__ sys, uint
 
 
 
+// The index data a gather warp will read for tile d (its row pointers, and
+// its block columns or, for CSR, its columns), prefetched into the L2 by the
+// producer a few tiles ahead, so that the gather warp's first, dependent
+// round trip is served from the L2 rather than from DRAM.
+__device__ __forceinline__ void prefetch_gather(const SpmvDesc &d) {
+    if (d.lng) return;
+    l2_prefetch(d.rptr, 4u * (d.nr + 1));
+    if (d.layout == LAYOUT_BSR6) l2_prefetch(d.cols, 4u * (d.k1 - d.k0));
+    else l2_prefetch(d.csrc, 4u * ((d.k1 - d.ka + 3) & ~3u));
+}
+
 // Producer warp of the SpMV ring. The warp resolves 32 work items at once
 // (one lane each: work item -> system -> tile), so the chain of dependent
 // loads behind a tile is paid once per 32 tiles, and keeps the work items of
@@ -699,6 +719,8 @@ __device__ __forceinline__ void spmv_producer(const SysDesc *__restrict__ sys, S
                     mbar_arrive(&meta[s]);  // the gather warps may start on this tile
                     issue_spmv(desc[s], smem + s * kSpmvStageFloats, &full[s], pol);
                     issued = k + 1;
+                    if (kSpmvPrefetchAhead > 0 && i + kSpmvPrefetchAhead < cnt)
+                        prefetch_gather(bdesc[i + kSpmvPrefetchAhead]);
                 } else {  // end marker
                     desc[s].valid = 0;
                     mbar_arrive(&meta[s]);

@@ -43,6 +43,12 @@ constexpr int kGatherWarps = WSB_GATHER_WARPS;
 #ifndef WSB_GATHER_KEEP_L2
 #define WSB_GATHER_KEEP_L2 0
 #endif
+// The SpMV producer prefetches the index data of the tile this many tiles
+// ahead of the one it issues into the L2 (0: no prefetch).
+#ifndef WSB_SPMV_PREFETCH_AHEAD
+#define WSB_SPMV_PREFETCH_AHEAD 0
+#endif
+constexpr uint32_t kSpmvPrefetchAhead = WSB_SPMV_PREFETCH_AHEAD;
 // 16-byte column loads each gather lane keeps in flight for a CSR tile.
 #ifndef WSB_CSR_GATHER_BATCH
 #define WSB_CSR_GATHER_BATCH 8
