@@ -42,11 +42,12 @@ def peaks():
 
 
 # DRAM bytes per algorithmic byte of the SpMV kernel, from one ncu capture of
-# k_spmv_loop on the 56^3 lattice (BSR6 tiles, 206 MB of matrix > L2):
-# dram__bytes_read.sum 184.363 MB + dram__bytes_write.sum 7.223 MB over
-# 188.285 MB of algorithmic bytes. The kernel streams every byte once, so the
-# traffic scales with the launch's algorithmic bytes.
-SPMV_DRAM_PER_ALGO_BYTE = (184.363008e6 + 7.222784e6) / 188285444.0
+# k_spmv_loop on the 56^3 lattice (BSR6 tiles, 206 MB of matrix > L2; see
+# profiles/k_spmv_loop_bsr6_side56.md): dram__bytes_read.sum 184.378112 MB +
+# dram__bytes_write.sum 4.038656 MB over 188.285444 MB of algorithmic bytes.
+# The kernel streams every byte once, so the traffic scales with the launch's
+# algorithmic bytes.
+SPMV_DRAM_PER_ALGO_BYTE = (184.378112e6 + 4.038656e6) / 188285444.0
 
 
 def spmv_traffic(algo_bytes):
