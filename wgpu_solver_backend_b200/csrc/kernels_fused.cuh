@@ -46,7 +46,7 @@ constexpr int kGatherWarps = WSB_GATHER_WARPS;
 // The SpMV producer prefetches the index data of the tile this many tiles
 // ahead of the one it issues into the L2 (0: no prefetch).
 #ifndef WSB_SPMV_PREFETCH_AHEAD
-#define WSB_SPMV_PREFETCH_AHEAD 0
+#define WSB_SPMV_PREFETCH_AHEAD 2
 #endif
 constexpr uint32_t kSpmvPrefetchAhead = WSB_SPMV_PREFETCH_AHEAD;
 // 16-byte column loads each gather lane keeps in flight for a CSR tile.
