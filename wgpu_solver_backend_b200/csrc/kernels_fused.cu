@@ -73,6 +73,17 @@ __device__ __forceinline__ void tma_load_stream(void *dst, const void *src, uint
         : "memory");
 }
 
+// Two FP32 products in one packed instruction (mul.rn.f32x2, sm_100): each
+// lane is rounded to nearest on its own, exactly as two __fmul_rn.
+__device__ __forceinline__ float2 mul2_rn(float2 a, float2 b) {
+    float2 r;
+    asm("{\n\t.reg .b64 ra, rb, rc;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rc, ra, rb;\n\tmov.b64 {%0, %1}, rc;\n}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+
 // Bulk prefetch of a global range into the L2 (no completion tracking). The
 // range is widened to 16-byte boundaries; every array it is used on has tail
 // padding, so the widened range stays inside its allocation.
@@ -503,12 +514,12 @@ __device__ __forceinline__ float csr_stage(const SpmvDesc &d, const float *stage
         uint32_t q = s;
         // Operands two products ahead, so shared-memory latency overlaps the add chain.
         for (; q + 4u <= e; q += 4u) {
-            const float v0 = val[q], v1 = val[q + 1], v2 = val[q + 2], v3 = val[q + 3];
-            const float x0 = xg[q], x1 = xg[q + 1], x2 = xg[q + 2], x3 = xg[q + 3];
-            acc = __fadd_rn(acc, __fmul_rn(v0, x0));
-            acc = __fadd_rn(acc, __fmul_rn(v1, x1));
-            acc = __fadd_rn(acc, __fmul_rn(v2, x2));
-            acc = __fadd_rn(acc, __fmul_rn(v3, x3));
+            const float2 p01 = mul2_rn(make_float2(val[q], val[q + 1]), make_float2(xg[q], xg[q + 1]));
+            const float2 p23 = mul2_rn(make_float2(val[q + 2], val[q + 3]), make_float2(xg[q + 2], xg[q + 3]));
+            acc = __fadd_rn(acc, p01.x);
+            acc = __fadd_rn(acc, p01.y);
+            acc = __fadd_rn(acc, p23.x);
+            acc = __fadd_rn(acc, p23.y);
         }
         for (; q < e; ++q) acc = __fadd_rn(acc, __fmul_rn(val[q], xg[q]));
     }
@@ -553,12 +564,15 @@ __device__ __forceinline__ float bsr_stage(const SpmvDesc &d, const float *stage
                 nb0 = B[0], nb1 = B[1], nb2 = B[2], nx0 = X[0], nx1 = X[1], nx2 = X[2];
                 if (kOwn) nc = bcol[blk + 1];
             }
-            acc = __fadd_rn(acc, __fmul_rn(b0.x, x0.x));
-            acc = __fadd_rn(acc, __fmul_rn(b0.y, x0.y));
-            acc = __fadd_rn(acc, __fmul_rn(b1.x, x1.x));
-            acc = __fadd_rn(acc, __fmul_rn(b1.y, x1.y));
-            acc = __fadd_rn(acc, __fmul_rn(b2.x, x2.x));
-            acc = __fadd_rn(acc, __fmul_rn(b2.y, x2.y));
+            // The six products (packed two at a time), then the adds in
+            // index order.
+            const float2 q0 = mul2_rn(b0, x0), q1 = mul2_rn(b1, x1), q2 = mul2_rn(b2, x2);
+            acc = __fadd_rn(acc, q0.x);
+            acc = __fadd_rn(acc, q0.y);
+            acc = __fadd_rn(acc, q1.x);
+            acc = __fadd_rn(acc, q1.y);
+            acc = __fadd_rn(acc, q2.x);
+            acc = __fadd_rn(acc, q2.y);
             if (kOwn && c == self) {
                 const float2 xs = a < 2u ? x0 : (a < 4u ? x1 : x2);
                 xo = (a & 1u) ? xs.y : xs.x;
