@@ -272,7 +272,7 @@ int prepare_system_device(Context *ctx, uint32_t n, const uint32_t *row_ptr, con
     M->tile_rows = caps.upd_rows;
     M->tile_blocks = caps.upd_blocks;
     std::vector<UpdTile> utiles;
-    build_upd_tiles_balanced(ctx, n, bs, nb, &utiles, caps.upd_rows, caps.upd_blocks);
+    build_upd_tiles(n, bs, nb, &utiles, caps.upd_rows, caps.upd_blocks);
     M->n_utiles = (uint32_t)utiles.size();
     if ((rc = dev_upload(ctx, &M->utiles, utiles.data(), utiles.size(), 1, st, &M->bytes))) {
         free_csr();
@@ -300,7 +300,7 @@ int prepare_system_device(Context *ctx, uint32_t n, const uint32_t *row_ptr, con
         A->bytes += sizeof(float) * (A->nbsr * 36 + kPadElems);
         k_prep_bsr6_fill<<<grid_of(6ull * nbr, 128, sms), 128, 0, st>>>(nbr, d_rp, d_col, d_val, A->bcol, A->bval);
         WSB_CUDA_TRY(ctx, cudaGetLastError());
-        build_spmv_tiles_balanced(ctx, LAYOUT_BSR6, n, brow_ptr.data(), &stiles, caps.spmv_rows, caps.spmv_cap);
+        build_spmv_tiles_bsr(nbr, brow_ptr.data(), &stiles, caps.spmv_rows / 6, caps.spmv_cap);
         A->h_rows = std::move(brow_ptr);
         free_csr();
     } else {
@@ -327,7 +327,7 @@ int prepare_system_device(Context *ctx, uint32_t n, const uint32_t *row_ptr, con
         WSB_CUDA_TRY(ctx, cudaMemcpyAsync(A->col, d_col, nz_bytes, cudaMemcpyDeviceToDevice, st));
         WSB_CUDA_TRY(ctx, cudaMemcpyAsync(A->val, d_val, nz_bytes, cudaMemcpyDeviceToDevice, st));
         free_csr();
-        build_spmv_tiles_balanced(ctx, LAYOUT_CSR, n, row_ptr, &stiles, caps.spmv_rows, caps.spmv_cap);
+        build_spmv_tiles_csr(n, row_ptr, &stiles, caps.spmv_rows, caps.spmv_cap);
         A->h_rows.assign(row_ptr, row_ptr + (size_t)n + 1);
     }
     A->tile_rows = caps.spmv_rows;

@@ -81,7 +81,7 @@ int upload_matA(Context *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_
         if ((rc = upload(ctx, &out->bval, bval.data(), bval.size(), 16, st, &out->bytes))) return rc;
         const TileCaps caps = tile_caps_for(LAYOUT_BSR6, n, nnz);
         std::vector<SpmvTile> tiles;
-        build_spmv_tiles_balanced(ctx, LAYOUT_BSR6, n, brow_ptr.data(), &tiles, caps.spmv_rows, caps.spmv_cap);
+        build_spmv_tiles_bsr(n / 6, brow_ptr.data(), &tiles, caps.spmv_rows / 6, caps.spmv_cap);
         out->h_rows = brow_ptr;
         out->tile_rows = caps.spmv_rows;
         out->tile_cap = caps.spmv_cap;
@@ -96,7 +96,7 @@ int upload_matA(Context *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_
     if ((rc = upload(ctx, &out->val, val, nnz, kPadElems, st, &out->bytes))) return rc;
     const TileCaps caps = tile_caps_for(LAYOUT_CSR, n, nnz);
     std::vector<SpmvTile> tiles;
-    build_spmv_tiles_balanced(ctx, LAYOUT_CSR, n, row_ptr, &tiles, caps.spmv_rows, caps.spmv_cap);
+    build_spmv_tiles_csr(n, row_ptr, &tiles, caps.spmv_rows, caps.spmv_cap);
     out->h_rows.assign(row_ptr, row_ptr + (size_t)n + 1);
     out->tile_rows = caps.spmv_rows;
     out->tile_cap = caps.spmv_cap;
@@ -104,91 +104,6 @@ int upload_matA(Context *ctx, uint32_t n, const uint32_t *row_ptr, const uint32_
     if ((rc = upload(ctx, &out->stiles, tiles.data(), tiles.size(), 1, st, &out->bytes))) return rc;
     WSB_CUDA_TRY(ctx, cudaStreamSynchronize(st));
     return WSB_OK;
-}
-
-namespace {
-
-// Resident CTAs of k_spmv_loop (which = 0) or k_update (which = 1) on the
-// context's device: the grid the engine launches for a system with at least
-// that many tiles.
-int resident_grid(Context *ctx, int which) {
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    if (ctx->resident_grid[which] == 0) {
-        int occ = 0;
-        cudaError_t e;
-        if (which == 0) {
-            cudaFuncSetAttribute(k_spmv_loop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpmvSmem);
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_spmv_loop, kSpmvThreads, kSpmvSmem);
-        } else {
-            cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdSmem);
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_update, kUpdThreads, kUpdSmem);
-        }
-        if (e != cudaSuccess) occ = 0;
-        ctx->resident_grid[which] = std::max(1, occ) * std::max(1, ctx->sm_count);
-    }
-    return ctx->resident_grid[which];
-}
-
-// The loop kernels walk their tiles with a grid-stride loop, so with T tiles
-// on G resident CTAs a launch lasts ceil(T/G) tile times while the average
-// CTA does T/G tiles: the 80^3 lattice's 4000 update tiles of 128 blocks on
-// 444 CTAs keep 4 CTAs busy for a tenth tile while the rest idle. Where a CTA
-// does at most 16 tiles, both caps (a, b; multiples of qa, qb) shrink by
-// T / (ceil(T/G) G), so that every CTA gets the same number of slightly
-// smaller tiles (a few quanta of slack when the first try still overshoots);
-// otherwise, or when no try fits, the tiling of the given caps stays.
-// build(a, b, &tiles) builds a tiling with caps a and b.
-template <class T, class Build>
-void balance_tiles(uint64_t G, uint32_t cap_a, uint32_t qa, uint32_t cap_b, uint32_t qb, Build build,
-                   std::vector<T> *out) {
-    build(cap_a, cap_b, out);
-    const uint64_t T0 = out->size();
-    if (T0 <= G || T0 % G == 0) return;
-    const uint64_t k = (T0 + G - 1) / G;
-    if (k > 16) return;
-    const uint64_t target = k * G;
-    const double f = (double)T0 / (double)target;
-    std::vector<T> t;
-    for (uint32_t extra = 0; extra < 4; ++extra) {
-        const uint32_t a = std::min<uint32_t>(cap_a, qa * ((uint32_t)std::ceil(cap_a * f / qa) + extra));
-        const uint32_t b = std::min<uint32_t>(cap_b, qb * ((uint32_t)std::ceil(cap_b * f / qb) + extra));
-        if (a >= cap_a && b >= cap_b) return;
-        build(a, b, &t);
-        if (t.size() <= target) {
-            out->swap(t);
-            return;
-        }
-    }
-}
-
-}  // namespace
-
-void build_upd_tiles_balanced(Context *ctx, uint32_t n, const uint32_t *bs, uint32_t nb, std::vector<UpdTile> *out,
-                              uint32_t max_rows, uint32_t max_blocks) {
-    max_rows = std::max<uint32_t>(6, std::min<uint32_t>(max_rows, kUpdTileRows));
-    max_blocks = std::max<uint32_t>(1, std::min<uint32_t>(max_blocks, kUpdBlocks));
-    balance_tiles(
-        (uint64_t)resident_grid(ctx, 1), max_rows, 6, max_blocks, 1,
-        [&](uint32_t r, uint32_t b, std::vector<UpdTile> *t) { build_upd_tiles(n, bs, nb, t, r, b); }, out);
-}
-
-void build_spmv_tiles_balanced(Context *ctx, uint32_t layout, uint32_t n, const uint32_t *rows,
-                               std::vector<SpmvTile> *out, uint32_t max_rows, uint32_t cap) {
-    const uint64_t G = (uint64_t)resident_grid(ctx, 0);
-    if (layout == LAYOUT_BSR6) {
-        const uint32_t br = std::max<uint32_t>(1, std::min<uint32_t>(max_rows / 6, kSpmvTileRows / 6));
-        cap = std::max<uint32_t>(1, std::min<uint32_t>(cap, kBsrCapBlocks));
-        balance_tiles(
-            G, br, 1, cap, 1,
-            [&](uint32_t a, uint32_t b, std::vector<SpmvTile> *t) { build_spmv_tiles_bsr(n / 6, rows, t, a, b); },
-            out);
-    } else {
-        max_rows = std::max<uint32_t>(1, std::min<uint32_t>(max_rows, kSpmvTileRows));
-        cap = std::max<uint32_t>(4, std::min<uint32_t>(cap, kCsrCap));
-        balance_tiles(
-            G, max_rows, 1, cap, 4,
-            [&](uint32_t a, uint32_t b, std::vector<SpmvTile> *t) { build_spmv_tiles_csr(n, rows, t, a, b); }, out);
-    }
 }
 
 int upload_precond(Context *ctx, uint32_t n, const float *lu, const uint32_t *bs, uint64_t bs_len, cudaStream_t st,
@@ -200,7 +115,7 @@ int upload_precond(Context *ctx, uint32_t n, const float *lu, const uint32_t *bs
     if ((rc = upload(ctx, &out->lu, lu, (size_t)out->nb * 36, 4, st, &out->bytes))) return rc;
     if ((rc = upload(ctx, &out->bs, bs, (size_t)bs_len, 8, st, &out->bytes))) return rc;
     std::vector<UpdTile> tiles;
-    build_upd_tiles_balanced(ctx, n, bs, out->nb, &tiles, kUpdTileRows, kUpdBlocks);
+    build_upd_tiles(n, bs, out->nb, &tiles, kUpdTileRows, kUpdBlocks);
     out->h_bs.assign(bs, bs + bs_len);
     out->tile_rows = kUpdTileRows;
     out->tile_blocks = kUpdBlocks;

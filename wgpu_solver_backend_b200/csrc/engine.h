@@ -63,14 +63,6 @@ void tile_caps_clear();
 // Rebuild a matrix's SpMV tiles or a preconditioner's update tiles with new
 // caps (device tile lists replaced; no solve may be running on them).
 int retile_spmv(MatA *A, uint32_t rows, uint32_t cap, cudaStream_t st);
-// Update tiles (at most max_rows rows and max_blocks blocks) and SpMV tiles
-// (rows: the CSR row_ptr or the BSR6 block-row pointer; caps as TileCaps),
-// shrunk evenly when that gives every CTA of the kernel's resident grid the
-// same number of tiles (engine.cu).
-void build_spmv_tiles_balanced(Context *ctx, uint32_t layout, uint32_t n, const uint32_t *rows,
-                               std::vector<SpmvTile> *out, uint32_t max_rows, uint32_t cap);
-void build_upd_tiles_balanced(Context *ctx, uint32_t n, const uint32_t *bs, uint32_t nb, std::vector<UpdTile> *out,
-                              uint32_t max_rows, uint32_t max_blocks);
 int retile_update(Precond *M, uint32_t rows, uint32_t blocks, cudaStream_t st);
 // Times candidate tilings of the matrix's SpMV and update kernels, keeps the
 // fastest of each and records them for the matrix's shape class (tune.cu).

@@ -83,7 +83,8 @@ void tile_caps_clear() {
 
 int retile_spmv(MatA *A, uint32_t rows, uint32_t cap, cudaStream_t st) {
     std::vector<SpmvTile> tiles;
-    build_spmv_tiles_balanced(A->ctx, A->layout, A->n, A->h_rows.data(), &tiles, rows, cap);
+    if (A->layout == LAYOUT_BSR6) build_spmv_tiles_bsr(A->n / 6, A->h_rows.data(), &tiles, rows / 6, cap);
+    else build_spmv_tiles_csr(A->n, A->h_rows.data(), &tiles, rows, cap);
     const int rc = upload_tiles(A->ctx, tiles, st, &A->stiles, &A->n_stiles, &A->bytes);
     if (!rc) {
         A->tile_rows = rows;
@@ -94,7 +95,7 @@ int retile_spmv(MatA *A, uint32_t rows, uint32_t cap, cudaStream_t st) {
 
 int retile_update(Precond *M, uint32_t rows, uint32_t blocks, cudaStream_t st) {
     std::vector<UpdTile> tiles;
-    build_upd_tiles_balanced(M->ctx, M->n, M->h_bs.data(), M->nb, &tiles, rows, blocks);
+    build_upd_tiles(M->n, M->h_bs.data(), M->nb, &tiles, rows, blocks);
     const int rc = upload_tiles(M->ctx, tiles, st, &M->utiles, &M->n_utiles, &M->bytes);
     if (!rc) {
         M->tile_rows = rows;

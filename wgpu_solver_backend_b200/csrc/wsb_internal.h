@@ -189,7 +189,6 @@ struct Context {
     cudaStream_t stream = nullptr;     // own_stream or the caller's
     cudaDeviceProp prop{};
     int sm_count = 0;
-    int resident_grid[2] = {0, 0};     // resident CTAs of k_spmv_loop, k_update (0: not yet queried)
     std::string last_error;
     std::mutex mu;
 };
