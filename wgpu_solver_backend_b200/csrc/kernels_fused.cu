@@ -84,24 +84,6 @@ __device__ __forceinline__ float2 mul2_rn(float2 a, float2 b) {
     return r;
 }
 
-__device__ __forceinline__ float2 add2_rn(float2 a, float2 b) {
-    float2 r;
-    asm("{\n\t.reg .b64 ra, rb, rc;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-        "add.rn.f32x2 rc, ra, rb;\n\tmov.b64 {%0, %1}, rc;\n}"
-        : "=f"(r.x), "=f"(r.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return r;
-}
-
-__device__ __forceinline__ float2 sub2_rn(float2 a, float2 b) {
-    float2 r;
-    asm("{\n\t.reg .b64 ra, rb, rc;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-        "sub.rn.f32x2 rc, ra, rb;\n\tmov.b64 {%0, %1}, rc;\n}"
-        : "=f"(r.x), "=f"(r.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return r;
-}
-
 // Bulk prefetch of a global range into the L2 (no completion tracking). The
 // range is widened to 16-byte boundaries; every array it is used on has tail
 // padding, so the widened range stays inside its allocation.
@@ -1038,25 +1020,19 @@ __device__ __forceinline__ void issue_upd(const UpdDesc &d, float *stage, uint64
 template <int kK>
 __device__ __forceinline__ float row_update(const UpdDesc &d, float *stage, uint32_t o) {
     if (kK == K_INIT) return __fsub_rn(stage[o], stage[3 * kVecCap + o]);
-    // (x, r) and (p, s) are updated as packed pairs (f32x2, each lane
-    // rounded on its own as the scalar operations would be).
-    const float2 am = make_float2(d.alpha, -d.alpha);
+    const float a = d.alpha, ma = -a;
     if (kK == K_LOOP) {
-        const float2 prod = mul2_rn(am, make_float2(stage[kVecCap + o], stage[3 * kVecCap + o]));
-        const float2 xr = add2_rn(make_float2(stage[o], stage[2 * kVecCap + o]), prod);
-        stage[o] = xr.x;
-        return xr.y;
+        const float ri = __fadd_rn(stage[2 * kVecCap + o], __fmul_rn(ma, stage[3 * kVecCap + o]));
+        stage[o] = __fadd_rn(stage[o], __fmul_rn(a, stage[kVecCap + o]));
+        return ri;
     }
-    const float2 uw = make_float2(stage[4 * kVecCap + o], stage[3 * kVecCap + o]);
-    const float2 ps = d.first ? uw
-                              : add2_rn(mul2_rn(make_float2(stage[kVecCap + o], stage[5 * kVecCap + o]),
-                                                make_float2(d.beta, d.beta)),
-                                        uw);
-    stage[kVecCap + o] = ps.x;
-    stage[5 * kVecCap + o] = ps.y;
-    const float2 xr = add2_rn(make_float2(stage[o], stage[2 * kVecCap + o]), mul2_rn(am, ps));
-    stage[o] = xr.x;
-    return xr.y;
+    const float u = stage[4 * kVecCap + o], w = stage[3 * kVecCap + o];
+    const float pi = d.first ? u : __fadd_rn(__fmul_rn(stage[kVecCap + o], d.beta), u);
+    const float si = d.first ? w : __fadd_rn(__fmul_rn(stage[5 * kVecCap + o], d.beta), w);
+    stage[kVecCap + o] = pi;
+    stage[5 * kVecCap + o] = si;
+    stage[o] = __fadd_rn(stage[o], __fmul_rn(a, pi));
+    return __fadd_rn(stage[2 * kVecCap + o], __fmul_rn(ma, si));
 }
 
 // Stage slot that receives the new z (u): slot 1 for the classic kernels (p
@@ -1105,39 +1081,23 @@ __device__ __forceinline__ void bj_block(const UpdDesc &d, float *stage, uint32_
         y[i] = 0.0f;
         xs[i] = 0.0f;
     }
-    // Forward solve by columns: once y[q] is known every later row subtracts
-    // L[i][q] y[q], so each row still subtracts in the order q = 0, 1, ...
-    // (block_jacobi.wgsl:93-101); two rows share one packed multiply and one
-    // packed subtract. Rows i >= m are computed but never used.
-    float t[6];
 #pragma unroll
-    for (int i = 0; i < 6; ++i) t[i] = rv[i];
+    for (int i = 0; i < 6; ++i) {
+        if ((uint32_t)i < m) {
+            float t = rv[i];
 #pragma unroll
-    for (int q = 0; q < 6; ++q) {
-        if ((uint32_t)q < m) {
-            y[q] = t[q];
-            const float yq = y[q];
-#pragma unroll
-            for (int i = q + 1; i < 6; i += 2) {
-                if (i + 1 < 6) {
-                    const float2 pr = mul2_rn(make_float2(L[i * 6 + q], L[(i + 1) * 6 + q]), make_float2(yq, yq));
-                    const float2 tt = sub2_rn(make_float2(t[i], t[i + 1]), pr);
-                    t[i] = tt.x;
-                    t[i + 1] = tt.y;
-                } else {
-                    t[i] = __fsub_rn(t[i], __fmul_rn(L[i * 6 + q], yq));
-                }
-            }
+            for (int q = 0; q < i; ++q) t = __fsub_rn(t, __fmul_rn(L[i * 6 + q], y[q]));
+            y[i] = t;
         }
     }
 #pragma unroll
     for (int i = 5; i >= 0; --i) {
         if ((uint32_t)i < m) {
-            float v = y[i];
+            float t = y[i];
 #pragma unroll
             for (int q = i + 1; q < 6; ++q)
-                if ((uint32_t)q < m) v = __fsub_rn(v, __fmul_rn(L[i * 6 + q], xs[q]));
-            xs[i] = __fdiv_rn(v, L[i * 6 + i]);
+                if ((uint32_t)q < m) t = __fsub_rn(t, __fmul_rn(L[i * 6 + q], xs[q]));
+            xs[i] = __fdiv_rn(t, L[i * 6 + i]);
         }
     }
 #pragma unroll
