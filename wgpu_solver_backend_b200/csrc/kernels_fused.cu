@@ -1157,18 +1157,19 @@ __device__ __forceinline__ double2 group_sum2(double a, double b, double *red, u
 }
 
 // Sum of n pairs of FP64 partials over the group: thread lt adds elements
-// lt, lt + GT, ... in that order (8 loads in flight), then the group sum.
+// lt, lt + GT, ... in that order (16 loads in flight: the last CTA's sum is
+// bound by the bytes it keeps in flight), then the group sum.
 template <int GT, int BAR>
 __device__ __forceinline__ double2 group_sum_partials2(const double2 *__restrict__ p, uint32_t n, double *red,
                                                        uint32_t lt) {
     double va = 0.0, vb = 0.0;
     uint32_t i = lt;
-    for (; i + 7u * GT < n; i += 8u * GT) {
-        double2 q[8];
+    for (; i + 15u * GT < n; i += 16u * GT) {
+        double2 q[16];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) q[u] = __ldcg(p + i + u * GT);
+        for (int u = 0; u < 16; ++u) q[u] = __ldcg(p + i + u * GT);
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
+        for (int u = 0; u < 16; ++u) {
             va += q[u].x;
             vb += q[u].y;
         }
