@@ -272,29 +272,6 @@ __device__ __forceinline__ double sum_partials(const double *__restrict__ p, uin
     return block_sum<N>(v, red);
 }
 
-// The same for pairs of partials (both components in one pass).
-template <int N = kThreads>
-__device__ __forceinline__ double2 sum_partials2(const double2 *__restrict__ p, uint32_t n, double *red) {
-    double va = 0.0, vb = 0.0;
-    uint32_t i = threadIdx.x;
-    for (; i + 7u * N < n; i += 8u * N) {
-        double2 q[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) q[u] = __ldcg(p + i + u * N);
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            va += q[u].x;
-            vb += q[u].y;
-        }
-    }
-    for (; i < n; i += N) {
-        const double2 q = __ldcg(p + i);
-        va += q.x;
-        vb += q.y;
-    }
-    return block_sum2<N>(va, vb, red);
-}
-
 // Ticket on a per-system counter: this CTA adds the number of tiles whose
 // partials it has published (thread `who` wrote them and takes the ticket);
 // true in every thread of the CTA whose tickets complete the system's total.
@@ -857,7 +834,14 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
         float acc, p_own = 0.0f;
         bool own_ok = false;
         if (bsr_gathered) {
-            acc = bsr_stage<kMode == M_LOOP>(d, stage, &p_own, &own_ok);
+            // The row's own p value for p.Ap is read from global memory (an L2
+            // hit: the gather has just read it) before the block walk, which
+            // then carries no per-block test for the diagonal block.
+            if (kMode == M_LOOP && tid < nrows) {
+                p_own = __ldg(d.x + row0 + tid);
+                own_ok = true;
+            }
+            acc = bsr_stage<false>(d, stage, nullptr, nullptr);
         } else {
             if (kMode == M_LOOP && tid < nrows) {
                 p_own = __ldg(d.x + row0 + tid);
