@@ -5,6 +5,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <queue>
+#include <vector>
 
 #include "engine.h"
 
@@ -151,6 +153,7 @@ struct Engine::Slot {
     float *s = nullptr;  // single reduction: s = A p
     double *x64 = nullptr, *part_a = nullptr, *hist = nullptr;
     double2 *part_b = nullptr;
+    uint32_t sgroups = 0, ugroups = 0;  // reduction groups of the SpMV and update tiles
     uint64_t hist_cap = 0;
     enum Phase { IDLE, NEED_INIT, RUNNING, NEED_REFINE, DONE } phase = IDLE;
     bool mixed = false;
@@ -363,6 +366,14 @@ int Engine::add(const MatA *A, const Precond *M, const SolveCfg &cfg, uint32_t *
     d.n_utiles = M->n_utiles;
     d.part_a = sl->part_a;
     d.part_b = sl->part_b;
+    // As many reduction groups as the kernel has resident CTAs (or one per
+    // tile): the last CTA of a reduction then sums at most one partial per
+    // CTA instead of one per tile. The groups depend only on the tile count
+    // and the device, so a system's sums are the same alone and batched.
+    sl->sgroups = std::min<uint32_t>(A->n_stiles, (uint32_t)max_grid_a_);
+    sl->ugroups = std::min<uint32_t>(M->n_utiles, (uint32_t)update_grid_max());
+    d.n_sgroups = sl->sgroups;
+    d.n_ugroups = sl->ugroups;
     d.st = d_state_ + s;
     d.history = sl->hist;
     d.algo = (uint32_t)cfg.algorithm;
@@ -429,28 +440,113 @@ void Engine::remove(uint32_t s) {
 // rewrites a region before the copy that feeds the next kernel reading it, so
 // a copy still pending from earlier in the same step carries either the same
 // content or content that a later copy replaces before any kernel reads it.
-int Engine::rebuild_work() {
-    size_t per = 1;
-    for (auto &s : slots_)
-        if (s) per += std::max<size_t>(std::max(s->A->n_stiles, s->M->n_utiles), chunks_of(s->A->n));
-    if (per > work_cap_) {
-        WSB_CUDA_TRY(ctx_, cudaStreamSynchronize(stream_));
-        const size_t nc = std::max(per, work_cap_ * 2);
-        cudaFree(d_work_);
-        cudaFreeHost(h_work_);
-        d_work_ = nullptr;
-        h_work_ = nullptr;
-        WSB_CUDA_TRY(ctx_, cudaMalloc(&d_work_, sizeof(WorkItem) * nc * kLists));
-        WSB_CUDA_TRY(ctx_, cudaMallocHost(&h_work_, sizeof(WorkItem) * nc * kLists));
-        work_cap_ = nc;
+namespace {
+
+struct GroupSrc {
+    uint32_t sys, tiles, groups;
+};
+
+// The tiles of some systems laid out in columns for the column walk of the
+// loop kernels (StepParams). A system of T tiles in G reduction groups has
+// group g = tiles g, g + G, g + 2G, ... (strided: CTAs that walk one group
+// each then sweep the system together, as a grid-stride loop would, which
+// keeps the DRAM streams and the reuse of x in the L2 of neighbouring tiles;
+// contiguous groups of T/G tiles measured slower). Groups go, largest first,
+// to the column holding the fewest tiles so far; a column lists its groups'
+// tiles in increasing order, the first and the last tile of each group
+// flagged.
+// out gets columns x (longest column) items, positions past the end of a
+// column marked kNoSys. Returns the number of columns (at most max_cols).
+uint32_t layout_groups(const std::vector<GroupSrc> &src, uint32_t max_cols, std::vector<WorkItem> *out) {
+    struct Grp {
+        uint32_t size, sys, g, stride;
+    };
+    std::vector<Grp> grps;
+    for (const GroupSrc &q : src)
+        for (uint32_t g = 0; g < q.groups; ++g) grps.push_back({(q.tiles - g + q.groups - 1) / q.groups, q.sys, g, q.groups});
+    out->clear();
+    const uint32_t w = (uint32_t)std::min<size_t>(grps.size(), std::max<uint32_t>(max_cols, 1u));
+    if (w == 0) return 0;
+    std::stable_sort(grps.begin(), grps.end(), [](const Grp &a, const Grp &b) { return a.size > b.size; });
+    std::vector<std::vector<WorkItem>> cols(w);
+    using Load = std::pair<uint64_t, uint32_t>;  // (tiles so far, column)
+    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+    for (uint32_t c = 0; c < w; ++c) heap.push({0, c});
+    for (const Grp &g : grps) {
+        const Load l = heap.top();
+        heap.pop();
+        for (uint32_t t = 0; t < g.size; ++t) {
+            const uint32_t fl = (t == 0 ? kGroupFirst : 0u) | (t + 1 == g.size ? kGroupLast : 0u);
+            cols[l.second].push_back({g.sys, g.g + t * g.stride, g.g, fl});
+        }
+        heap.push({l.first + g.size, l.second});
     }
-    uint32_t na = 0, nb = 0, nch = 0;
+    size_t len = 0;
+    for (const auto &c : cols) len = std::max(len, c.size());
+    out->assign((size_t)w * len, WorkItem{kNoSys, 0u, 0u, 0u});
+    for (uint32_t c = 0; c < w; ++c)
+        for (size_t j = 0; j < cols[c].size(); ++j) (*out)[c + (size_t)w * j] = cols[c][j];
+    return w;
+}
+
+}  // namespace
+
+// Grows the list storage to at least `per` items per list, keeping every
+// list's contents (host and device).
+int Engine::ensure_work_cap(size_t per) {
+    if (per <= work_cap_) return WSB_OK;
+    WSB_CUDA_TRY(ctx_, cudaStreamSynchronize(stream_));
+    const size_t nc = std::max(per, work_cap_ * 2);
+    WorkItem *d = nullptr, *h = nullptr;
+    WSB_CUDA_TRY(ctx_, cudaMalloc(&d, sizeof(WorkItem) * nc * kLists));
+    const cudaError_t he = cudaMallocHost(&h, sizeof(WorkItem) * nc * kLists);
+    if (he != cudaSuccess) {
+        cudaFree(d);
+        return fail(ctx_, WSB_ERR_OUT_OF_MEMORY, "pinned work-list allocation failed: %s", cudaGetErrorString(he));
+    }
+    if (work_cap_) {
+        for (int l = 0; l < kLists; ++l) {
+            std::memcpy(h + l * nc, h_work_ + l * work_cap_, sizeof(WorkItem) * work_cap_);
+            const cudaError_t ce = cudaMemcpy(d + l * nc, d_work_ + l * work_cap_, sizeof(WorkItem) * work_cap_,
+                                              cudaMemcpyDeviceToDevice);
+            if (ce != cudaSuccess) {
+                cudaFree(d);
+                cudaFreeHost(h);
+                return fail(ctx_, WSB_ERR_CUDA, "work-list copy failed: %s", cudaGetErrorString(ce));
+            }
+        }
+    }
+    cudaFree(d_work_);
+    cudaFreeHost(h_work_);
+    d_work_ = d;
+    h_work_ = h;
+    work_cap_ = nc;
+    return WSB_OK;
+}
+
+int Engine::rebuild_work() {
+    std::vector<GroupSrc> ga, gb;
+    size_t per = 1;
+    for (uint32_t s = 0; s < slots_.size(); ++s) {
+        const Slot *sl = slots_[s].get();
+        if (!sl) continue;
+        per += std::max<size_t>(std::max(sl->A->n_stiles, sl->M->n_utiles), chunks_of(sl->A->n));
+        if (sl->phase != Slot::RUNNING) continue;
+        ga.push_back({s, sl->A->n_stiles, sl->sgroups});
+        gb.push_back({s, sl->M->n_utiles, sl->ugroups});
+    }
+    std::vector<WorkItem> la, lb;
+    w_work_a_ = layout_groups(ga, (uint32_t)max_grid_a_, &la);
+    w_work_b_ = layout_groups(gb, (uint32_t)update_grid_max(), &lb);
+    int rc = ensure_work_cap(std::max(per, std::max(la.size(), lb.size()) + 1));
+    if (rc) return rc;
+    uint32_t na = (uint32_t)la.size(), nb = (uint32_t)lb.size(), nch = 0;
     WorkItem *wa = h_work_ + L_A * work_cap_, *wb = h_work_ + L_B * work_cap_, *wc = h_work_ + L_C * work_cap_;
+    if (na) std::memcpy(wa, la.data(), sizeof(WorkItem) * na);
+    if (nb) std::memcpy(wb, lb.data(), sizeof(WorkItem) * nb);
     for (uint32_t s = 0; s < slots_.size(); ++s) {
         const Slot *sl = slots_[s].get();
         if (!sl || sl->phase != Slot::RUNNING) continue;
-        for (uint32_t t = 0; t < sl->A->n_stiles; ++t) wa[na++] = {s, t};
-        for (uint32_t t = 0; t < sl->M->n_utiles; ++t) wb[nb++] = {s, t};
         for (uint32_t t = 0; t < chunks_of(sl->A->n); ++t) wc[nch++] = {s, t};
     }
     n_work_a_ = na;
@@ -526,13 +622,21 @@ int Engine::capture_loop(uint32_t ga, uint32_t gb, uint32_t gc) {
 }
 
 int Engine::launch_init(const std::vector<uint32_t> &ids) {
-    WorkItem *ia = h_work_ + L_IA * work_cap_, *ib = h_work_ + L_IB * work_cap_;
-    uint32_t na = 0, nb = 0;
+    std::vector<GroupSrc> ga, gb;
     for (uint32_t s : ids) {
         const Slot &sl = *slots_[s];
-        for (uint32_t t = 0; t < sl.A->n_stiles; ++t) ia[na++] = {s, t};
-        for (uint32_t t = 0; t < sl.M->n_utiles; ++t) ib[nb++] = {s, t};
+        ga.push_back({s, sl.A->n_stiles, sl.sgroups});
+        gb.push_back({s, sl.M->n_utiles, sl.ugroups});
     }
+    std::vector<WorkItem> la, lb;
+    h_sp_->w_init_a = layout_groups(ga, (uint32_t)max_grid_a_, &la);
+    h_sp_->w_init_b = layout_groups(gb, (uint32_t)max_grid_b_, &lb);
+    int rc = ensure_work_cap(std::max(la.size(), lb.size()) + 1);
+    if (rc) return rc;
+    WorkItem *ia = h_work_ + L_IA * work_cap_, *ib = h_work_ + L_IB * work_cap_;
+    const uint32_t na = (uint32_t)la.size(), nb = (uint32_t)lb.size();
+    if (na) std::memcpy(ia, la.data(), sizeof(WorkItem) * na);
+    if (nb) std::memcpy(ib, lb.data(), sizeof(WorkItem) * nb);
     if (na) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + L_IA * work_cap_, ia, sizeof(WorkItem) * na, cudaMemcpyHostToDevice, stream_));
     if (nb) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + L_IB * work_cap_, ib, sizeof(WorkItem) * nb, cudaMemcpyHostToDevice, stream_));
     h_sp_->n_init_a = na;
@@ -670,6 +774,8 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
     fill_list_ptrs();
     h_sp_->n_work_a = n_work_a_;
     h_sp_->n_work_b = n_work_b_;
+    h_sp_->w_work_a = w_work_a_;
+    h_sp_->w_work_b = w_work_b_;
     h_sp_->n_work_c = n_work_c_;
     h_sp_->error = 0;
     h_sp_->wait_cycles = ctx_->wait_cycles;
@@ -689,8 +795,8 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
     h_sp_->loop_limit = limit;
     WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_sp_, h_sp_, sizeof(StepParams), cudaMemcpyHostToDevice, stream_));
     if (!init.empty()) {
-        const uint32_t ga = std::min<uint32_t>(h_sp_->n_init_a, (uint32_t)max_grid_a_);
-        const uint32_t gb = std::min<uint32_t>(h_sp_->n_init_b, (uint32_t)max_grid_b_);
+        const uint32_t ga = std::min<uint32_t>(h_sp_->w_init_a, (uint32_t)max_grid_a_);
+        const uint32_t gb = std::min<uint32_t>(h_sp_->w_init_b, (uint32_t)max_grid_b_);
         const SysDesc *dsys = d_sys_;
         StepParams *dsp = d_sp_;
         if (ga) WSB_CUDA_TRY(ctx_, launch_pdl(k_spmv_init, ga, kSpmvThreads, kSpmvSmem, stream_, dsys, dsp));
@@ -698,8 +804,8 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
         launches_ += (ga ? 1 : 0) + (gb ? 1 : 0);
     }
     if (num_active_ > 0 && n_work_a_ > 0) {
-        const uint32_t ga = std::max<uint32_t>(1, std::min<uint32_t>(n_work_a_, (uint32_t)max_grid_a_));
-        const uint32_t gb = std::max<uint32_t>(1, std::min<uint32_t>(n_work_b_, (uint32_t)update_grid_max()));
+        const uint32_t ga = std::max<uint32_t>(1, std::min<uint32_t>(w_work_a_, (uint32_t)max_grid_a_));
+        const uint32_t gb = std::max<uint32_t>(1, std::min<uint32_t>(w_work_b_, (uint32_t)update_grid_max()));
         const uint32_t gc = std::max<uint32_t>(1, std::min<uint32_t>(n_work_c_, (uint32_t)max_grid_c_));
         if (use_graph_) {
             if (!exec_ || ga > graph_grid_a_ || gb > graph_grid_b_ || gc > graph_grid_c_ || 2 * ga < graph_grid_a_ ||
@@ -811,6 +917,8 @@ int Engine::profile_kernels(uint32_t s, uint32_t iters, double ms[5]) {
     fill_list_ptrs();
     h_sp_->n_work_a = n_work_a_;
     h_sp_->n_work_b = n_work_b_;
+    h_sp_->w_work_a = w_work_a_;
+    h_sp_->w_work_b = w_work_b_;
     h_sp_->n_work_c = n_work_c_;
     h_sp_->error = 0;
     h_sp_->wait_cycles = ctx_->wait_cycles;
@@ -818,11 +926,11 @@ int Engine::profile_kernels(uint32_t s, uint32_t iters, double ms[5]) {
     h_sp_->loop_count = 0;
     h_sp_->loop_limit = iters;
     WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_sp_, h_sp_, sizeof(StepParams), cudaMemcpyHostToDevice, stream_));
-    const uint32_t ga = std::min<uint32_t>(n_work_a_, (uint32_t)max_grid_a_);
-    const uint32_t gb = std::min<uint32_t>(n_work_b_, (uint32_t)update_grid_max());
+    const uint32_t ga = std::min<uint32_t>(w_work_a_, (uint32_t)max_grid_a_);
+    const uint32_t gb = std::min<uint32_t>(w_work_b_, (uint32_t)update_grid_max());
     const uint32_t gc = std::min<uint32_t>(n_work_c_, (uint32_t)max_grid_c_);
-    k_spmv_init<<<std::min<uint32_t>(h_sp_->n_init_a, (uint32_t)max_grid_a_), kSpmvThreads, kSpmvSmem, stream_>>>(d_sys_, d_sp_);
-    k_init<<<std::min<uint32_t>(h_sp_->n_init_b, (uint32_t)max_grid_b_), kUpdThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
+    k_spmv_init<<<std::max<uint32_t>(1, std::min<uint32_t>(h_sp_->w_init_a, (uint32_t)max_grid_a_)), kSpmvThreads, kSpmvSmem, stream_>>>(d_sys_, d_sp_);
+    k_init<<<std::max<uint32_t>(1, std::min<uint32_t>(h_sp_->w_init_b, (uint32_t)max_grid_b_)), kUpdThreads, kUpdSmem, stream_>>>(d_sys_, d_sp_);
     std::vector<cudaEvent_t> ev(4 * (size_t)iters);
     for (auto &e : ev) WSB_CUDA_TRY(ctx_, cudaEventCreate(&e));
     for (uint32_t i = 0; i < iters; ++i) {

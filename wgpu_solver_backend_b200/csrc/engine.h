@@ -163,6 +163,8 @@ class Engine {
     WorkItem *d_work_ = nullptr, *h_work_ = nullptr;  // kLists regions
     size_t work_cap_ = 0;
     uint32_t n_work_a_ = 0, n_work_b_ = 0, n_work_c_ = 0;
+    uint32_t w_work_a_ = 0, w_work_b_ = 0;  // column counts of the loop SpMV and update lists
+    int ensure_work_cap(size_t per);
     bool work_dirty_ = true;
     bool use_graph_ = true;   // WSB_LOOP=launch: plain launches + host polling
     cudaGraph_t graph_ = nullptr;

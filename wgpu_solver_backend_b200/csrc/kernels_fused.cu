@@ -294,6 +294,25 @@ __device__ __forceinline__ bool take_ticket(uint32_t *counter, uint32_t cnt, uin
 // ---------------------------------------------------------------------------
 enum SpmvMode { M_LOOP = 0, M_INIT = 1, M_PLAIN = 2 };
 
+// The list positions a CTA takes, in order. A list of n items laid out in w
+// columns (StepParams) is walked column by column: columns blockIdx.x,
+// blockIdx.x + gridDim.x, ..., each from its first position (c) to its last
+// (c + w (n/w - 1)). w == 0: plain grid-stride over n items.
+constexpr uint32_t kNoPos = 0xffffffffu;
+struct ListWalk {
+    uint32_t n, w;
+    __device__ __forceinline__ uint32_t pos(uint32_t k) const {
+        if (w == 0) {
+            const uint64_t p = blockIdx.x + (uint64_t)k * gridDim.x;
+            return p < n ? (uint32_t)p : kNoPos;
+        }
+        const uint32_t len = n / w;
+        if (len == 0) return kNoPos;
+        const uint64_t c = blockIdx.x + (uint64_t)(k / len) * gridDim.x;
+        return c < w ? (uint32_t)(c + (uint64_t)w * (k % len)) : kNoPos;
+    }
+};
+
 // Stage layout (floats), from kernels_fused.cuh: CSR values [0, kCsrCap+8),
 // the gathered x[col] of every staged value at kColOff (same index as the
 // value); BSR6 block values [0, 36 kBsrCapBlocks), block columns
@@ -318,7 +337,9 @@ struct SpmvDesc {
     uint32_t lng;     // a single row longer than a stage: synchronous path
     const float *x;   // the vector multiplied: p (loop), x0 (init) or the caller's x
     float *y;         // Ap (loop, init) or the caller's y
-    double *part;     // the system's per-tile p.Ap partials (loop)
+    double *part;     // the system's per-group p.Ap partials (loop)
+    uint32_t grp;     // the tile's reduction group
+    uint32_t gflags;  // kGroupFirst / kGroupLast
     const uint32_t *rptr;  // the tile's row pointers: row_ptr + r0 or brow_ptr + r0
     const uint32_t *cols;  // BSR6: the tile's block columns, bcol + k0
     const float *vsrc;     // bulk-copy source of the values: bval + 36 k0, or val + ka
@@ -338,13 +359,16 @@ __device__ __forceinline__ const float *spmv_input(const SysDesc &S, const float
 // the (system, tile) the index stands for.
 template <int kMode>
 __device__ __forceinline__ bool check_spmv(const SysDesc *__restrict__ sys, const StepParams *sp, uint32_t idx,
-                                           uint32_t nw, WorkItem *it) {
-    if (idx >= nw) return false;
+                                           WorkItem *it) {
+    if (idx == kNoPos) return false;
     if (kMode == M_PLAIN) {
         it->sys = 0;
         it->tile = idx;
+        it->grp = 0;
+        it->flags = 0;
         return true;
     }
+    if (it->sys == kNoSys) return false;  // a position that carries no tile
     if (it->sys >= sp->num_sys || it->tile >= sys[it->sys].n_stiles) {
         atomicOr(const_cast<uint32_t *>(&sp->error), kErrBadItem);  // invalid work item: skipped
         return false;
@@ -373,6 +397,8 @@ __device__ __forceinline__ void fill_spmv(const SysDesc *__restrict__ sys, WorkI
     d->x = spmv_input<kMode>(S, xplain);
     d->y = kMode == M_PLAIN ? yplain : S.ap;
     d->part = S.part_a;
+    d->grp = it.grp;
+    d->gflags = it.flags;
     d->rptr = (bsr ? S.brow_ptr : S.row_ptr) + T.row0;
     d->cols = bsr ? S.bcol + T.k0 : nullptr;
     d->vsrc = bsr ? S.bval + (size_t)T.k0 * 36u : S.val + ka;
@@ -446,7 +472,6 @@ __device__ __forceinline__ void gather_tile(const SpmvDesc &d, float *stage, uin
     }
     const float *__restrict__ xin = d.x;
     const bool al8 = (reinterpret_cast<uintptr_t>(xin) & 7u) == 0;
-    uint32_t *bcol = reinterpret_cast<uint32_t *>(stage + kBcolOff);
     float *xg = stage + kXgOff;
     const uint32_t nb = d.k1 - d.k0;
     // All block columns of this lane first (independent loads), then the
@@ -462,7 +487,6 @@ __device__ __forceinline__ void gather_tile(const SpmvDesc &d, float *stage, uin
     for (int q = 0; q < kPer; ++q) {
         const uint32_t blk = lane + 32u * q;
         if (blk < nb) {
-            bcol[blk] = c[q];
             const float *src = xin + 6u * (size_t)c[q];
             float *dst = xg + 6u * blk;
             if (al8) {
@@ -506,40 +530,31 @@ __device__ __forceinline__ float csr_stage(const SpmvDesc &d, const float *stage
 // BSR6 tile from a filled and gathered stage: thread t owns row (t/6, t%6) of
 // the tile and walks its block row's blocks in column order, six products
 // each from shared memory, added in index order (for complete 6x6 blocks
-// with sorted columns this is the CSR order). With kOwn, the thread also
-// picks its own row's x value out of the diagonal block's gathered x (for
-// p.Ap without another global load); *own_ok is false when the block row
-// has no diagonal block.
-template <bool kOwn>
-__device__ __forceinline__ float bsr_stage(const SpmvDesc &d, const float *stage, float *own, bool *own_ok) {
+// with sorted columns this is the CSR order). (The row's own p value for
+// p.Ap is loaded by the caller: testing every block for the diagonal one
+// cost the 80^3 SpMV 6 % of its time.)
+__device__ __forceinline__ float bsr_stage(const SpmvDesc &d, const float *stage) {
     const uint32_t *rp = reinterpret_cast<const uint32_t *>(stage + kRpOff);
-    const uint32_t *bcol = reinterpret_cast<const uint32_t *>(stage + kBcolOff);
     const float2 *xg = reinterpret_cast<const float2 *>(stage + kXgOff);
-    float acc = 0.0f, xo = 0.0f;
-    bool found = false;
+    float acc = 0.0f;
     const uint32_t t = threadIdx.x;
     if (t < 6u * d.nr) {
         const uint32_t br = t / 6u, a = t - 6u * br;
         const uint32_t s0 = rp[br] - d.k0, s1 = rp[br + 1] - d.k0;
-        const uint32_t self = d.r0 + br;
         // The next block's operands are loaded before this block's products
         // are added, so shared-memory latency overlaps the add chain.
         float2 b0, b1, b2, x0, x1, x2;
-        uint32_t c = 0;
         if (s0 < s1) {
             const float2 *B = reinterpret_cast<const float2 *>(stage + s0 * 36u + a * 6u);
             const float2 *X = xg + s0 * 3u;
             b0 = B[0], b1 = B[1], b2 = B[2], x0 = X[0], x1 = X[1], x2 = X[2];
-            if (kOwn) c = bcol[s0];
         }
         for (uint32_t blk = s0; blk < s1; ++blk) {
             float2 nb0 = b0, nb1 = b1, nb2 = b2, nx0 = x0, nx1 = x1, nx2 = x2;
-            uint32_t nc = c;
             if (blk + 1 < s1) {
                 const float2 *B = reinterpret_cast<const float2 *>(stage + (blk + 1) * 36u + a * 6u);
                 const float2 *X = xg + (blk + 1) * 3u;
                 nb0 = B[0], nb1 = B[1], nb2 = B[2], nx0 = X[0], nx1 = X[1], nx2 = X[2];
-                if (kOwn) nc = bcol[blk + 1];
             }
             // The six products (packed two at a time), then the adds in
             // index order.
@@ -550,17 +565,8 @@ __device__ __forceinline__ float bsr_stage(const SpmvDesc &d, const float *stage
             acc = __fadd_rn(acc, q1.y);
             acc = __fadd_rn(acc, q2.x);
             acc = __fadd_rn(acc, q2.y);
-            if (kOwn && c == self) {
-                const float2 xs = a < 2u ? x0 : (a < 4u ? x1 : x2);
-                xo = (a & 1u) ? xs.y : xs.x;
-                found = true;
-            }
-            b0 = nb0, b1 = nb1, b2 = nb2, x0 = nx0, x1 = nx1, x2 = nx2, c = nc;
+            b0 = nb0, b1 = nb1, b2 = nb2, x0 = nx0, x1 = nx1, x2 = nx2;
         }
-    }
-    if (kOwn) {
-        *own = xo;
-        *own_ok = found;
     }
     return acc;
 }
@@ -624,7 +630,7 @@ __device__ __forceinline__ void flush_spmv(const SysDesc *__restrict__ sys, uint
     const SysDesc &S = sys[s];
     SysState *st = S.st;
     if (!take_ticket<NC>(&st->cnt_a, cnt, S.n_stiles, s_last, kPublisher)) return;
-    const double pap = sum_partials<NC>(S.part_a, S.n_stiles, red);
+    const double pap = sum_partials<NC>(S.part_a, S.n_sgroups, red);
     if (threadIdx.x == 0) {
         if (S.algo == ALGO_SINGLE_REDUCTION) {
             const double gamma = st->rz_old;
@@ -677,23 +683,26 @@ __device__ __forceinline__ void spmv_producer(const SysDesc *__restrict__ sys, S
                                               long long lim) {
     constexpr uint32_t NS = kSpmvStages;
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t G = gridDim.x;
-    const uint32_t nw = kMode == M_PLAIN ? sys[0].n_stiles : kMode == M_INIT ? sp->n_init_a : sp->n_work_a;
+    const ListWalk walk = kMode == M_PLAIN  ? ListWalk{sys[0].n_stiles, 0u}
+                          : kMode == M_INIT ? ListWalk{sp->n_init_a, sp->w_init_a}
+                                            : ListWalk{sp->n_work_a, sp->w_work_a};
     const WorkItem *__restrict__ work = kMode == M_INIT ? sp->init_a : sp->work_a;
-    uint32_t base = blockIdx.x;  // work index of lane 0's item in the current batch
-    WorkItem it = {0u, 0u};
-    if (kMode != M_PLAIN && base + lane * G < nw) it = work[base + lane * G];
+    uint32_t base = 0;  // walk index of lane 0's item in the current batch
+    uint32_t ipos = walk.pos(lane);
+    WorkItem it = {0u, 0u, 0u, 0u};
+    if (kMode != M_PLAIN && ipos != kNoPos) it = work[ipos];
     uint32_t k = 0, issued = 0;
     bool err = false;
     const uint64_t pol = l2_evict_first_policy();
     for (;;) {
-        const bool ok = check_spmv<kMode>(sys, sp, base + lane * G, nw, &it);
+        const bool ok = check_spmv<kMode>(sys, sp, ipos, &it);
         const uint32_t m = __ballot_sync(0xffffffffu, ok);
         if (ok) fill_spmv<kMode>(sys, it, xplain, yplain, &bdesc[__popc(m & ((1u << lane) - 1u))]);
         const uint32_t cnt = __popc(m);
-        base += 32u * G;
-        const bool more = base < nw;
-        if (kMode != M_PLAIN && base + lane * G < nw) it = work[base + lane * G];  // next batch, in flight
+        base += 32u;
+        const bool more = walk.pos(base) != kNoPos;
+        ipos = walk.pos(base + lane);
+        if (kMode != M_PLAIN && ipos != kNoPos) it = work[ipos];  // next batch, in flight
         __syncwarp();
         if (lane == 0) {
             // After the last tile: one end marker for each gather warp.
@@ -796,7 +805,10 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
         return;
     }
     uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles of run_sys published since the last ticket
-    double *pend_part = nullptr;                  // publisher: partial slot of the tile in wred
+    // Publisher: the previous tile's group partial array (null: nothing
+    // pending), group and flags; the running sum of the current group.
+    double *pend_part = nullptr, gacc = 0.0;
+    uint32_t pend_grp = 0, pend_flags = 0;
     for (uint32_t k = 0;; ++k) {
         const uint32_t s = k % NS, par = (k / NS) & 1u;
         // Thread 0 waits (bounded) and shares the outcome through a flag that
@@ -818,7 +830,11 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
             double v = 0.0;
 #pragma unroll
             for (int q = 0; q < NC / 32; ++q) v += wr[q];
-            *pend_part = v;
+            // The tiles of a group come one after another in this CTA's walk:
+            // their partials are added in tile order, and the group's sum is
+            // stored with its last tile.
+            gacc = (pend_flags & kGroupFirst) ? v : gacc + v;
+            if (pend_flags & kGroupLast) pend_part[pend_grp] = gacc;
             pend_part = nullptr;
         }
         if (!d.valid) break;
@@ -831,22 +847,13 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
         const uint32_t row0 = d.layout == LAYOUT_BSR6 ? 6u * d.r0 : d.r0;
         const uint32_t nrows = d.layout == LAYOUT_BSR6 ? 6u * d.nr : d.nr;
         const bool bsr_gathered = !d.lng && d.layout == LAYOUT_BSR6;
+        // The row's own p value for p.Ap, read before the row's sum (an L2
+        // hit: the gather has just read it).
         float acc, p_own = 0.0f;
-        bool own_ok = false;
+        if (kMode == M_LOOP && tid < nrows) p_own = __ldg(d.x + row0 + tid);
         if (bsr_gathered) {
-            // The row's own p value for p.Ap is read from global memory (an L2
-            // hit: the gather has just read it) before the block walk, which
-            // then carries no per-block test for the diagonal block.
-            if (kMode == M_LOOP && tid < nrows) {
-                p_own = __ldg(d.x + row0 + tid);
-                own_ok = true;
-            }
-            acc = bsr_stage<false>(d, stage, nullptr, nullptr);
+            acc = bsr_stage(d, stage);
         } else {
-            if (kMode == M_LOOP && tid < nrows) {
-                p_own = __ldg(d.x + row0 + tid);
-                own_ok = true;
-            }
             if (d.lng) {
                 acc = long_tile(sys[d.sys], d, d.x, stage);
                 // That path wrote into the stage: order those writes before
@@ -857,8 +864,8 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
             }
         }
         float *const yv = d.y;
-        const float *const xv = d.x;
-        double *const part_slot = d.part + d.tile;
+        double *const part_arr = d.part;
+        const uint32_t tgrp = d.grp, tflags = d.gflags;
         // Done reading the stage: hand it back to the producer.
         mbar_arrive_warp(&empty[s]);
         if (kMode == M_PLAIN) {
@@ -868,15 +875,14 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
             if (tid < nrows) {
                 const uint32_t i = row0 + tid;
                 yv[i] = acc;
-                if (kMode == M_LOOP) {
-                    if (!own_ok) p_own = __ldg(xv + i);  // a block row without a diagonal block
-                    part = (double)p_own * (double)acc;
-                }
+                if (kMode == M_LOOP) part = (double)p_own * (double)acc;
             }
             if (kMode == M_LOOP) {
                 part = warp_sum(part);
                 if ((tid & 31u) == 0) wred[(NC / 32) * (k & 1u) + (tid >> 5)] = part;
-                pend_part = part_slot;
+                pend_part = part_arr;
+                pend_grp = tgrp;
+                pend_flags = tflags;
                 ++run_cnt;
             }
         }
@@ -917,7 +923,9 @@ struct UpdDesc {
     float beta;       // single reduction: the system's beta
     uint32_t first;   // single reduction: the system's first iteration (p = u, s = w)
     float *x, *r, *z, *p, *s;
-    double2 *part;    // the system's per-tile (r.r, r.z) partials
+    double2 *part;    // the system's per-group (r.r, r.z) partials
+    uint32_t grp;     // the tile's reduction group
+    uint32_t gflags;  // kGroupFirst / kGroupLast
     const float *v[6];  // bulk-copy sources of the staged vector slots (from ra)
     const float *lu;    // bulk-copy source of the tile's LU blocks
     const uint32_t *bs; // bulk-copy source of the tile's block starts (from ba)
@@ -928,8 +936,8 @@ struct UpdDesc {
 // for a system that is no longer active.
 template <int kK>
 __device__ __forceinline__ bool check_upd(const SysDesc *__restrict__ sys, const StepParams *sp, uint32_t idx,
-                                          uint32_t nw, WorkItem it) {
-    if (idx >= nw) return false;
+                                          WorkItem it) {
+    if (idx == kNoPos || it.sys == kNoSys) return false;
     if (it.sys >= sp->num_sys || it.tile >= sys[it.sys].n_utiles) {
         atomicOr(const_cast<uint32_t *>(&sp->error), kErrBadItem);  // invalid work item: skipped
         return false;
@@ -961,6 +969,8 @@ __device__ __forceinline__ void fill_upd(const SysDesc *__restrict__ sys, WorkIt
     d->p = S.p;
     d->s = S.s;
     d->part = S.part_b;
+    d->grp = it.grp;
+    d->gflags = it.flags;
     d->v[0] = (kK == K_INIT ? S.b : S.x) + ra;
     d->v[1] = S.p + ra;
     d->v[2] = S.r + ra;
@@ -1196,7 +1206,7 @@ __device__ __forceinline__ void flush_upd(const SysDesc *__restrict__ sys, StepP
     const SysDesc &S = sys[s];
     SysState *st = S.st;
     if (!group_ticket<GT, BAR>(&st->cnt_b, cnt, S.n_utiles, s_last, lt)) return;
-    const double2 sum = group_sum_partials2<GT, BAR>(S.part_b, S.n_utiles, red, lt);
+    const double2 sum = group_sum_partials2<GT, BAR>(S.part_b, S.n_ugroups, red, lt);
     if (lt != 0) return;
     if (kK == K_INIT) {
         st->bb = sum.x;
@@ -1254,23 +1264,24 @@ __device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, St
                                              long long lim) {
     constexpr uint32_t NS = kUpdStages;
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t G = gridDim.x;
-    const uint32_t nw = kK == K_INIT ? sp->n_init_b : sp->n_work_b;
+    const ListWalk walk = kK == K_INIT ? ListWalk{sp->n_init_b, sp->w_init_b} : ListWalk{sp->n_work_b, sp->w_work_b};
     const WorkItem *__restrict__ work = kK == K_INIT ? sp->init_b : sp->work_b;
-    uint32_t base = blockIdx.x;
-    WorkItem it = {0u, 0u};
-    if (base + lane * G < nw) it = work[base + lane * G];
+    uint32_t base = 0;  // walk index of lane 0's item in the current batch
+    uint32_t ipos = walk.pos(lane);
+    WorkItem it = {0u, 0u, 0u, 0u};
+    if (ipos != kNoPos) it = work[ipos];
     uint32_t k = 0, issued = 0;
     bool err = false;
     const uint64_t pol = l2_evict_first_policy();
     for (;;) {
-        const bool ok = check_upd<kK>(sys, sp, base + lane * G, nw, it);
+        const bool ok = check_upd<kK>(sys, sp, ipos, it);
         const uint32_t m = __ballot_sync(0xffffffffu, ok);
         if (ok) fill_upd<kK>(sys, it, &bdesc[__popc(m & ((1u << lane) - 1u))]);
         const uint32_t cnt = __popc(m);
-        base += 32u * G;
-        const bool more = base < nw;
-        if (base + lane * G < nw) it = work[base + lane * G];  // next batch, in flight
+        base += 32u;
+        const bool more = walk.pos(base) != kNoPos;
+        ipos = walk.pos(base + lane);
+        if (ipos != kNoPos) it = work[ipos];  // next batch, in flight
         __syncwarp();
         if (lane == 0) {
             // After the last tile: one end marker for the consumers.
@@ -1321,6 +1332,7 @@ __device__ __forceinline__ void upd_consumers(const SysDesc *__restrict__ sys, S
     constexpr int BAR = 1;
     const uint32_t lt = threadIdx.x;
     uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles of run_sys published since the last ticket
+    double2 gacc = make_double2(0.0, 0.0);  // thread 0: running (r.r, r.z) sum of the current group
     for (uint32_t k = 0;; ++k) {
         const uint32_t s = k % NS, par = (k / NS) & 1u;
         if (lt == 0) s_ok[k & 1u] = mbar_wait(&full[s], par, lim) ? 1 : 0;
@@ -1380,7 +1392,10 @@ __device__ __forceinline__ void upd_consumers(const SysDesc *__restrict__ sys, S
                 va += wred[q].x;
                 vb += wred[q].y;
             }
-            d.part[d.tile] = make_double2(va, vb);
+            // A group's tiles come one after another in this CTA's walk: its
+            // partials are added in tile order and stored with its last tile.
+            gacc = (d.gflags & kGroupFirst) ? make_double2(va, vb) : make_double2(gacc.x + va, gacc.y + vb);
+            if (d.gflags & kGroupLast) d.part[d.grp] = gacc;
         }
         // The consumers wrote into the stage: order those writes before the
         // bulk copies that will next fill it, then hand it back.

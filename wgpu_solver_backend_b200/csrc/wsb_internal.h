@@ -82,9 +82,15 @@ struct SpmvTile {
 struct UpdTile {
     uint32_t row0, row1, blk0, blk1;
 };
+// One tile of a system. In the SpMV and update lists the item also names the
+// tile's reduction group (grp) and whether the tile opens (kGroupFirst) and/or
+// closes (kGroupLast) it; a list position that carries no tile has sys ==
+// kNoSys (the list is laid out in columns, see StepParams).
 struct WorkItem {
-    uint32_t sys, tile;
+    uint32_t sys, tile, grp, flags;
 };
+constexpr uint32_t kNoSys = 0xffffffffu;
+constexpr uint32_t kGroupFirst = 1u, kGroupLast = 2u;
 
 // Mutable per-system scalars; written only by the last CTA of a reduction.
 struct alignas(64) SysState {
@@ -116,8 +122,9 @@ struct SysDesc {
     const SpmvTile *stiles;
     const UpdTile *utiles;
     uint32_t n_stiles, n_utiles;
-    double *part_a;                    // n_stiles partials
-    double2 *part_b;                   // n_utiles partial pairs
+    uint32_t n_sgroups, n_ugroups;     // reduction groups of the SpMV and update tiles
+    double *part_a;                    // p.Ap (u.w) partial of each SpMV tile group
+    double2 *part_b;                   // (r.r, r.z) partials of each update tile group (refinement: of each tile)
     SysState *st;
     double *history;                   // hist_cap entries or null
     uint32_t algo, pad_algo;           // Algo
@@ -150,6 +157,13 @@ struct StepParams {
     const WorkItem *aux_b;             // refinement kernels: update tiles
     uint32_t n_work_a, n_work_b, n_work_c;
     uint32_t n_init_a, n_init_b;
+    // Column counts of the grouped lists (loop and init SpMV / update lists):
+    // a list of n items is w columns of n / w consecutive positions each
+    // (position c + w j is item j of column c); a CTA walks columns
+    // blockIdx.x, blockIdx.x + gridDim.x, ..., each from its first item to
+    // its last, so a reduction group (consecutive items of one column) is
+    // always processed by one CTA, in order, whatever the grid.
+    uint32_t w_work_a, w_work_b, w_init_a, w_init_b;
     uint32_t n_aux_b;
     uint32_t num_active;               // systems still iterating
     uint32_t loop_count;               // body executions in this launch
