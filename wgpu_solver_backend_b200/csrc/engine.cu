@@ -451,42 +451,53 @@ struct GroupSrc {
 // group g = tiles g, g + G, g + 2G, ... (strided: CTAs that walk one group
 // each then sweep the system together, as a grid-stride loop would, which
 // keeps the DRAM streams and the reuse of x in the L2 of neighbouring tiles;
-// contiguous groups of T/G tiles measured slower). Groups go, largest first,
-// to the column holding the fewest tiles so far; a column lists its groups'
-// tiles in increasing order, the first and the last tile of each group
-// flagged.
-// out gets columns x (longest column) items, positions past the end of a
-// column marked kNoSys. Returns the number of columns (at most max_cols).
-uint32_t layout_groups(const std::vector<GroupSrc> &src, uint32_t max_cols, std::vector<WorkItem> *out) {
-    struct Grp {
-        uint32_t size, sys, g, stride;
-    };
-    std::vector<Grp> grps;
-    for (const GroupSrc &q : src)
-        for (uint32_t g = 0; g < q.groups; ++g) grps.push_back({(q.tiles - g + q.groups - 1) / q.groups, q.sys, g, q.groups});
-    out->clear();
-    const uint32_t w = (uint32_t)std::min<size_t>(grps.size(), std::max<uint32_t>(max_cols, 1u));
-    if (w == 0) return 0;
-    std::stable_sort(grps.begin(), grps.end(), [](const Grp &a, const Grp &b) { return a.size > b.size; });
-    std::vector<std::vector<WorkItem>> cols(w);
-    using Load = std::pair<uint64_t, uint32_t>;  // (tiles so far, column)
-    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
-    for (uint32_t c = 0; c < w; ++c) heap.push({0, c});
-    for (const Grp &g : grps) {
-        const Load l = heap.top();
-        heap.pop();
-        for (uint32_t t = 0; t < g.size; ++t) {
-            const uint32_t fl = (t == 0 ? kGroupFirst : 0u) | (t + 1 == g.size ? kGroupLast : 0u);
-            cols[l.second].push_back({g.sys, g.g + t * g.stride, g.g, fl});
-        }
-        heap.push({l.first + g.size, l.second});
+// contiguous groups of T/G tiles measured slower). The groups of the
+// systems, in order, go round-robin to the columns (a system's groups differ
+// in size by at most one tile, so the columns stay balanced); a column lists
+// its groups' tiles in increasing order, the first and the last tile of each
+// group flagged, and positions past the end of a column are marked kNoSys.
+// The layout is rebuilt whenever the active set changes, so it is two
+// linear passes with no sorting: layout_size gives the columns (at most
+// max_cols) and the longest column, layout_fill writes w x len items.
+struct ColLayout {
+    uint32_t w = 0, len = 0;
+};
+
+uint32_t group_size(const GroupSrc &q, uint32_t g) { return (q.tiles - g + q.groups - 1) / q.groups; }
+
+ColLayout layout_size(const std::vector<GroupSrc> &src, uint32_t max_cols, std::vector<uint32_t> *col_len) {
+    uint64_t groups = 0;
+    for (const GroupSrc &q : src) groups += q.groups;
+    ColLayout l;
+    l.w = (uint32_t)std::min<uint64_t>(groups, std::max<uint32_t>(max_cols, 1u));
+    if (l.w == 0) return l;
+    col_len->assign(l.w, 0u);
+    uint32_t off = 0;
+    for (const GroupSrc &q : src) {
+        for (uint32_t g = 0; g < q.groups; ++g) (*col_len)[(off + g) % l.w] += group_size(q, g);
+        off = (uint32_t)((off + (uint64_t)q.groups) % l.w);
     }
-    size_t len = 0;
-    for (const auto &c : cols) len = std::max(len, c.size());
-    out->assign((size_t)w * len, WorkItem{kNoSys, 0u, 0u, 0u});
-    for (uint32_t c = 0; c < w; ++c)
-        for (size_t j = 0; j < cols[c].size(); ++j) (*out)[c + (size_t)w * j] = cols[c][j];
-    return w;
+    for (uint32_t c : *col_len) l.len = std::max(l.len, c);
+    return l;
+}
+
+void layout_fill(const std::vector<GroupSrc> &src, const ColLayout &l, std::vector<uint32_t> *cur, WorkItem *dst) {
+    if (l.w == 0) return;
+    const size_t n = (size_t)l.w * l.len;
+    for (size_t i = 0; i < n; ++i) dst[i] = WorkItem{kNoSys, 0u, 0u, 0u};
+    cur->assign(l.w, 0u);
+    uint32_t off = 0;
+    for (const GroupSrc &q : src) {
+        for (uint32_t g = 0; g < q.groups; ++g) {
+            const uint32_t c = (off + g) % l.w, sz = group_size(q, g);
+            uint32_t &j = (*cur)[c];
+            for (uint32_t t = 0; t < sz; ++t, ++j) {
+                const uint32_t fl = (t == 0 ? kGroupFirst : 0u) | (t + 1 == sz ? kGroupLast : 0u);
+                dst[c + (size_t)l.w * j] = WorkItem{q.sys, g + t * q.groups, g, fl};
+            }
+        }
+        off = (uint32_t)((off + (uint64_t)q.groups) % l.w);
+    }
 }
 
 }  // namespace
@@ -535,15 +546,17 @@ int Engine::rebuild_work() {
         ga.push_back({s, sl->A->n_stiles, sl->sgroups});
         gb.push_back({s, sl->M->n_utiles, sl->ugroups});
     }
-    std::vector<WorkItem> la, lb;
-    w_work_a_ = layout_groups(ga, (uint32_t)max_grid_a_, &la);
-    w_work_b_ = layout_groups(gb, (uint32_t)update_grid_max(), &lb);
-    int rc = ensure_work_cap(std::max(per, std::max(la.size(), lb.size()) + 1));
+    const ColLayout la = layout_size(ga, (uint32_t)max_grid_a_, &layout_tmp_);
+    const ColLayout lb = layout_size(gb, (uint32_t)update_grid_max(), &layout_tmp_);
+    const uint32_t na = la.w * la.len, nb = lb.w * lb.len;
+    int rc = ensure_work_cap(std::max<size_t>(per, std::max(na, nb) + 1));
     if (rc) return rc;
-    uint32_t na = (uint32_t)la.size(), nb = (uint32_t)lb.size(), nch = 0;
+    uint32_t nch = 0;
     WorkItem *wa = h_work_ + L_A * work_cap_, *wb = h_work_ + L_B * work_cap_, *wc = h_work_ + L_C * work_cap_;
-    if (na) std::memcpy(wa, la.data(), sizeof(WorkItem) * na);
-    if (nb) std::memcpy(wb, lb.data(), sizeof(WorkItem) * nb);
+    layout_fill(ga, la, &layout_tmp_, wa);
+    layout_fill(gb, lb, &layout_tmp_, wb);
+    w_work_a_ = la.w;
+    w_work_b_ = lb.w;
     for (uint32_t s = 0; s < slots_.size(); ++s) {
         const Slot *sl = slots_[s].get();
         if (!sl || sl->phase != Slot::RUNNING) continue;
@@ -628,15 +641,16 @@ int Engine::launch_init(const std::vector<uint32_t> &ids) {
         ga.push_back({s, sl.A->n_stiles, sl.sgroups});
         gb.push_back({s, sl.M->n_utiles, sl.ugroups});
     }
-    std::vector<WorkItem> la, lb;
-    h_sp_->w_init_a = layout_groups(ga, (uint32_t)max_grid_a_, &la);
-    h_sp_->w_init_b = layout_groups(gb, (uint32_t)max_grid_b_, &lb);
-    int rc = ensure_work_cap(std::max(la.size(), lb.size()) + 1);
+    const ColLayout la = layout_size(ga, (uint32_t)max_grid_a_, &layout_tmp_);
+    const ColLayout lb = layout_size(gb, (uint32_t)max_grid_b_, &layout_tmp_);
+    const uint32_t na = la.w * la.len, nb = lb.w * lb.len;
+    int rc = ensure_work_cap(std::max(na, nb) + 1);
     if (rc) return rc;
     WorkItem *ia = h_work_ + L_IA * work_cap_, *ib = h_work_ + L_IB * work_cap_;
-    const uint32_t na = (uint32_t)la.size(), nb = (uint32_t)lb.size();
-    if (na) std::memcpy(ia, la.data(), sizeof(WorkItem) * na);
-    if (nb) std::memcpy(ib, lb.data(), sizeof(WorkItem) * nb);
+    layout_fill(ga, la, &layout_tmp_, ia);
+    layout_fill(gb, lb, &layout_tmp_, ib);
+    h_sp_->w_init_a = la.w;
+    h_sp_->w_init_b = lb.w;
     if (na) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + L_IA * work_cap_, ia, sizeof(WorkItem) * na, cudaMemcpyHostToDevice, stream_));
     if (nb) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + L_IB * work_cap_, ib, sizeof(WorkItem) * nb, cudaMemcpyHostToDevice, stream_));
     h_sp_->n_init_a = na;

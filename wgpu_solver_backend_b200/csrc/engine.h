@@ -165,6 +165,7 @@ class Engine {
     uint32_t n_work_a_ = 0, n_work_b_ = 0, n_work_c_ = 0;
     uint32_t w_work_a_ = 0, w_work_b_ = 0;  // column counts of the loop SpMV and update lists
     int ensure_work_cap(size_t per);
+    std::vector<uint32_t> layout_tmp_;  // scratch of the work-list layout (column lengths / cursors)
     bool work_dirty_ = true;
     bool use_graph_ = true;   // WSB_LOOP=launch: plain launches + host polling
     cudaGraph_t graph_ = nullptr;
