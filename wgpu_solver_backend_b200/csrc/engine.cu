@@ -463,8 +463,6 @@ struct ColLayout {
     uint32_t w = 0, len = 0;
 };
 
-uint32_t group_size(const GroupSrc &q, uint32_t g) { return (q.tiles - g + q.groups - 1) / q.groups; }
-
 ColLayout layout_size(const std::vector<GroupSrc> &src, uint32_t max_cols, std::vector<uint32_t> *col_len) {
     uint64_t groups = 0;
     for (const GroupSrc &q : src) groups += q.groups;
@@ -472,32 +470,37 @@ ColLayout layout_size(const std::vector<GroupSrc> &src, uint32_t max_cols, std::
     l.w = (uint32_t)std::min<uint64_t>(groups, std::max<uint32_t>(max_cols, 1u));
     if (l.w == 0) return l;
     col_len->assign(l.w, 0u);
-    uint32_t off = 0;
+    uint32_t *len = col_len->data(), c = 0;
     for (const GroupSrc &q : src) {
-        for (uint32_t g = 0; g < q.groups; ++g) (*col_len)[(off + g) % l.w] += group_size(q, g);
-        off = (uint32_t)((off + (uint64_t)q.groups) % l.w);
+        const uint32_t base = q.tiles / q.groups, rem = q.tiles % q.groups;  // group g has base + (g < rem) tiles
+        for (uint32_t g = 0; g < q.groups; ++g) {
+            len[c] += base + (g < rem ? 1u : 0u);
+            if (++c == l.w) c = 0;
+        }
     }
-    for (uint32_t c : *col_len) l.len = std::max(l.len, c);
+    for (uint32_t i = 0; i < l.w; ++i) l.len = std::max(l.len, len[i]);
     return l;
 }
 
 void layout_fill(const std::vector<GroupSrc> &src, const ColLayout &l, std::vector<uint32_t> *cur, WorkItem *dst) {
     if (l.w == 0) return;
-    const size_t n = (size_t)l.w * l.len;
-    for (size_t i = 0; i < n; ++i) dst[i] = WorkItem{kNoSys, 0u, 0u, 0u};
     cur->assign(l.w, 0u);
-    uint32_t off = 0;
+    uint32_t *cj = cur->data(), c = 0;
+    const size_t w = l.w;
     for (const GroupSrc &q : src) {
+        const uint32_t base = q.tiles / q.groups, rem = q.tiles % q.groups;
         for (uint32_t g = 0; g < q.groups; ++g) {
-            const uint32_t c = (off + g) % l.w, sz = group_size(q, g);
-            uint32_t &j = (*cur)[c];
-            for (uint32_t t = 0; t < sz; ++t, ++j) {
-                const uint32_t fl = (t == 0 ? kGroupFirst : 0u) | (t + 1 == sz ? kGroupLast : 0u);
-                dst[c + (size_t)l.w * j] = WorkItem{q.sys, g + t * q.groups, g, fl};
-            }
+            const uint32_t sz = base + (g < rem ? 1u : 0u);
+            uint32_t j = cj[c];
+            WorkItem *o = dst + c + w * j;
+            for (uint32_t t = 0; t < sz; ++t, ++j, o += w)
+                *o = WorkItem{q.sys, g + t * q.groups, g, (t == 0 ? kGroupFirst : 0u) | (t + 1 == sz ? kGroupLast : 0u)};
+            cj[c] = j;
+            if (++c == l.w) c = 0;
         }
-        off = (uint32_t)((off + (uint64_t)q.groups) % l.w);
     }
+    for (uint32_t cc = 0; cc < l.w; ++cc)
+        for (uint32_t j = cj[cc]; j < l.len; ++j) dst[cc + w * j] = WorkItem{kNoSys, 0u, 0u, 0u};
 }
 
 }  // namespace
@@ -660,7 +663,9 @@ int Engine::launch_init(const std::vector<uint32_t> &ids) {
 
 int Engine::launch_aux(const std::vector<uint32_t> &ids, int which) {
     if (ids.empty()) return WSB_OK;
-    int rc = rebuild_work();  // make sure storage exists
+    size_t need = 1;
+    for (uint32_t s : ids) need += slots_[s]->M->n_utiles;
+    int rc = ensure_work_cap(need);  // the loop lists stay as they are
     if (rc) return rc;
     WorkItem *xb = h_work_ + L_X * work_cap_;
     uint32_t nb = 0;
@@ -707,7 +712,10 @@ int Engine::finish_slot(uint32_t s, int status) {
 
 int Engine::step(uint32_t loop_limit, bool *any_left) {
     int rc;
-    if ((rc = rebuild_work())) return rc;  // ensures storage even with nothing running
+    // The lists change only when the active set does (work_dirty_); the
+    // layout is not free (a linear pass over every tile of every active
+    // system), so it is not redone every step.
+    if ((work_dirty_ || work_cap_ == 0) && (rc = rebuild_work())) return rc;
     const bool timing = true;
     if (timing) cudaEventRecord(ev0_, stream_);
     // 1) Mixed precision: refinement sweeps (x64 += d; r64 = b - A x64).
