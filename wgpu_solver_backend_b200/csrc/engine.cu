@@ -283,6 +283,9 @@ int Engine::add(const MatA *A, const Precond *M, const SolveCfg &cfg, uint32_t *
         return fail(ctx_, WSB_ERR_UNSUPPORTED,
                     "systems iterated together use one recurrence: this batch or server already runs algorithm %u",
                     algo_);
+    // The lists may still name stopped systems (their tiles skipped); a
+    // slot they name must not take a new system before they are re-laid out.
+    if (retired_tiles_) work_dirty_ = true;
     uint32_t s = (uint32_t)slots_.size();
     for (uint32_t i = 0; i < slots_.size(); ++i)
         if (!slots_[i]) {
@@ -568,6 +571,10 @@ int Engine::rebuild_work() {
     n_work_a_ = na;
     n_work_b_ = nb;
     n_work_c_ = nch;
+    listed_tiles_ = 0;
+    for (const GroupSrc &q : ga) listed_tiles_ += q.tiles;
+    for (const GroupSrc &q : gb) listed_tiles_ += q.tiles;
+    retired_tiles_ = 0;
     if (na) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + L_A * work_cap_, wa, sizeof(WorkItem) * na, cudaMemcpyHostToDevice, stream_));
     if (nb) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + L_B * work_cap_, wb, sizeof(WorkItem) * nb, cudaMemcpyHostToDevice, stream_));
     if (nch) WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(d_work_ + L_C * work_cap_, wc, sizeof(WorkItem) * nch, cudaMemcpyHostToDevice, stream_));
@@ -885,7 +892,10 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
         sl.iters_total += st.iter;
         sl.out.rr = st.rr;
         sl.out.breakdown = (int)st.breakdown;
-        work_dirty_ = true;
+        // Its device state is inactive, so the kernels skip its tiles: the
+        // lists are re-laid out only once a quarter of their tiles belong to
+        // systems that stopped (or when one joins), not at every retirement.
+        retired_tiles_ += (uint64_t)sl.A->n_stiles + sl.M->n_utiles;
         if (sl.mixed) {
             if (st.status == ST_BREAKDOWN) sl.stalled = true;
             if (st.status == ST_MAXITER && sl.iters_total >= sl.cfg.max_iter) sl.stalled = true;
@@ -897,6 +907,7 @@ int Engine::step(uint32_t loop_limit, bool *any_left) {
         }
     }
     (void)body_iters;
+    if (retired_tiles_ * 4 > listed_tiles_) work_dirty_ = true;
     WSB_CUDA_TRY(ctx_, cudaMemcpyAsync(h_sp_rb_, d_sp_, sizeof(StepParams), cudaMemcpyDeviceToHost, stream_));
     WSB_CUDA_TRY(ctx_, cudaStreamSynchronize(stream_));
     // Graph: the gate kernel once, then three body kernels per loop pass.

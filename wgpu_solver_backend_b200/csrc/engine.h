@@ -166,6 +166,7 @@ class Engine {
     uint32_t w_work_a_ = 0, w_work_b_ = 0;  // column counts of the loop SpMV and update lists
     int ensure_work_cap(size_t per);
     std::vector<uint32_t> layout_tmp_;  // scratch of the work-list layout (column lengths / cursors)
+    uint64_t listed_tiles_ = 0, retired_tiles_ = 0;  // tiles in the lists; of systems stopped since
     bool work_dirty_ = true;
     bool use_graph_ = true;   // WSB_LOOP=launch: plain launches + host polling
     cudaGraph_t graph_ = nullptr;
