@@ -457,8 +457,9 @@ struct GroupSrc {
 // contiguous groups of T/G tiles measured slower). The groups of the
 // systems, in order, go round-robin to the columns (a system's groups differ
 // in size by at most one tile, so the columns stay balanced); a column lists
-// its groups' tiles in increasing order, the first and the last tile of each
-// group flagged, and positions past the end of a column are marked kNoSys.
+// its groups' tiles in increasing order (the kernels derive a tile's group
+// and its place in it from the tile index), and positions past the end of a
+// column are marked kNoSys.
 // The layout is rebuilt whenever the active set changes, so it is two
 // linear passes with no sorting: layout_size gives the columns (at most
 // max_cols) and the longest column, layout_fill writes w x len items.
@@ -496,14 +497,13 @@ void layout_fill(const std::vector<GroupSrc> &src, const ColLayout &l, std::vect
             const uint32_t sz = base + (g < rem ? 1u : 0u);
             uint32_t j = cj[c];
             WorkItem *o = dst + c + w * j;
-            for (uint32_t t = 0; t < sz; ++t, ++j, o += w)
-                *o = WorkItem{q.sys, g + t * q.groups, g, (t == 0 ? kGroupFirst : 0u) | (t + 1 == sz ? kGroupLast : 0u)};
+            for (uint32_t t = 0; t < sz; ++t, ++j, o += w) *o = WorkItem{q.sys, g + t * q.groups};
             cj[c] = j;
             if (++c == l.w) c = 0;
         }
     }
     for (uint32_t cc = 0; cc < l.w; ++cc)
-        for (uint32_t j = cj[cc]; j < l.len; ++j) dst[cc + w * j] = WorkItem{kNoSys, 0u, 0u, 0u};
+        for (uint32_t j = cj[cc]; j < l.len; ++j) dst[cc + w * j] = WorkItem{kNoSys, 0u};
 }
 
 }  // namespace

@@ -377,8 +377,6 @@ __device__ __forceinline__ bool check_spmv(const SysDesc *__restrict__ sys, cons
     if (kMode == M_PLAIN) {
         it->sys = 0;
         it->tile = idx;
-        it->grp = 0;
-        it->flags = 0;
         return true;
     }
     if (it->sys == kNoSys) return false;  // a position that carries no tile
@@ -410,8 +408,14 @@ __device__ __forceinline__ void fill_spmv(const SysDesc *__restrict__ sys, WorkI
     d->x = spmv_input<kMode>(S, xplain);
     d->y = kMode == M_PLAIN ? yplain : S.ap;
     d->part = S.part_a;
-    d->grp = it.grp;
-    d->gflags = it.flags;
+    if (kMode == M_LOOP) {
+        const uint32_t G = S.n_sgroups;
+        d->grp = it.tile % G;
+        d->gflags = (it.tile < G ? kGroupFirst : 0u) | (it.tile + G >= S.n_stiles ? kGroupLast : 0u);
+    } else {
+        d->grp = 0;
+        d->gflags = 0;
+    }
     d->rptr = (bsr ? S.brow_ptr : S.row_ptr) + T.row0;
     d->cols = bsr ? S.bcol + T.k0 : nullptr;
     d->vsrc = bsr ? S.bval + (size_t)T.k0 * 36u : S.val + ka;
@@ -702,7 +706,7 @@ __device__ __forceinline__ void spmv_producer(const SysDesc *__restrict__ sys, S
     const WorkItem *__restrict__ work = kMode == M_INIT ? sp->init_a : sp->work_a;
     uint32_t base = 0;  // walk index of lane 0's item in the current batch
     uint32_t ipos = walk.pos(lane);
-    WorkItem it = {0u, 0u, 0u, 0u};
+    WorkItem it = {0u, 0u};
     if (kMode != M_PLAIN && ipos != kNoPos) it = work[ipos];
     uint32_t k = 0, issued = 0;
     bool err = false;
@@ -983,8 +987,11 @@ __device__ __forceinline__ void fill_upd(const SysDesc *__restrict__ sys, WorkIt
     d->p = S.p;
     d->s = S.s;
     d->part = S.part_b;
-    d->grp = it.grp;
-    d->gflags = it.flags;
+    {
+        const uint32_t G = S.n_ugroups;
+        d->grp = it.tile % G;
+        d->gflags = (it.tile < G ? kGroupFirst : 0u) | (it.tile + G >= S.n_utiles ? kGroupLast : 0u);
+    }
     d->v[0] = (kK == K_INIT ? S.b : S.x) + ra;
     d->v[1] = S.p + ra;
     d->v[2] = S.r + ra;
@@ -1282,7 +1289,7 @@ __device__ __forceinline__ void upd_producer(const SysDesc *__restrict__ sys, St
     const WorkItem *__restrict__ work = kK == K_INIT ? sp->init_b : sp->work_b;
     uint32_t base = 0;  // walk index of lane 0's item in the current batch
     uint32_t ipos = walk.pos(lane);
-    WorkItem it = {0u, 0u, 0u, 0u};
+    WorkItem it = {0u, 0u};
     if (ipos != kNoPos) it = work[ipos];
     uint32_t k = 0, issued = 0;
     bool err = false;

@@ -82,12 +82,13 @@ struct SpmvTile {
 struct UpdTile {
     uint32_t row0, row1, blk0, blk1;
 };
-// One tile of a system. In the SpMV and update lists the item also names the
-// tile's reduction group (grp) and whether the tile opens (kGroupFirst) and/or
-// closes (kGroupLast) it; a list position that carries no tile has sys ==
-// kNoSys (the list is laid out in columns, see StepParams).
+// One tile of a system (a list position that carries no tile has sys ==
+// kNoSys; the SpMV and update lists are laid out in columns, see
+// StepParams). A tile's reduction group and whether it opens or closes it
+// follow from the tile index: with G groups, tile t is in group t mod G,
+// opens it when t < G and closes it when t + G >= T.
 struct WorkItem {
-    uint32_t sys, tile, grp, flags;
+    uint32_t sys, tile;
 };
 constexpr uint32_t kNoSys = 0xffffffffu;
 constexpr uint32_t kGroupFirst = 1u, kGroupLast = 2u;
