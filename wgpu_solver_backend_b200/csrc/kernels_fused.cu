@@ -822,10 +822,13 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
         return;
     }
     uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles of run_sys published since the last ticket
-    // Publisher: the previous tile's group partial array (null: nothing
-    // pending), group and flags; the running sum of the current group.
-    double *pend_part = nullptr, gacc = 0.0;
-    uint32_t pend_grp = 0, pend_flags = 0;
+    // Publisher: the group partial array of the group the previous tile
+    // closed (null: nothing pending) and the group. Every thread: its rows'
+    // p.Ap products summed over the current group's tiles (which come one
+    // after another in this CTA's walk), so that the FP64 warp and CTA sums
+    // run once per group, not once per tile.
+    double *pend_part = nullptr, gpart = 0.0;
+    uint32_t pend_grp = 0;
     for (uint32_t k = 0;; ++k) {
         const uint32_t s = k % NS, par = (k / NS) & 1u;
         // Thread 0 waits (bounded) and shares the outcome through a flag that
@@ -841,17 +844,14 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
         // The descriptor is read in place: it stays valid until this stage
         // is handed back; what is needed after that is copied first.
         const SpmvDesc &d = desc[s];
-        // The previous tile's p.Ap partial: its warps' sums in warp order.
+        // The group that the previous tile closed: its warps' sums in warp
+        // order.
         if (kMode == M_LOOP && tid == kPublisher && pend_part) {
             const double *wr = wred + (NC / 32) * ((k - 1) & 1u);
             double v = 0.0;
 #pragma unroll
             for (int q = 0; q < NC / 32; ++q) v += wr[q];
-            // The tiles of a group come one after another in this CTA's walk:
-            // their partials are added in tile order, and the group's sum is
-            // stored with its last tile.
-            gacc = (pend_flags & kGroupFirst) ? v : gacc + v;
-            if (pend_flags & kGroupLast) pend_part[pend_grp] = gacc;
+            pend_part[pend_grp] = v;
             pend_part = nullptr;
         }
         if (!d.valid) break;
@@ -895,11 +895,13 @@ __device__ __forceinline__ void spmv_pipeline(const SysDesc *__restrict__ sys, S
                 if (kMode == M_LOOP) part = (double)p_own * (double)acc;
             }
             if (kMode == M_LOOP) {
-                part = warp_sum(part);
-                if ((tid & 31u) == 0) wred[(NC / 32) * (k & 1u) + (tid >> 5)] = part;
-                pend_part = part_arr;
-                pend_grp = tgrp;
-                pend_flags = tflags;
+                gpart = (tflags & kGroupFirst) ? part : gpart + part;
+                if (tflags & kGroupLast) {
+                    const double w = warp_sum(gpart);
+                    if ((tid & 31u) == 0) wred[(NC / 32) * (k & 1u) + (tid >> 5)] = w;
+                    pend_part = part_arr;
+                    pend_grp = tgrp;
+                }
                 ++run_cnt;
             }
         }
@@ -1353,7 +1355,7 @@ __device__ __forceinline__ void upd_consumers(const SysDesc *__restrict__ sys, S
     constexpr int BAR = 1;
     const uint32_t lt = threadIdx.x;
     uint32_t run_sys = 0xffffffffu, run_cnt = 0;  // tiles of run_sys published since the last ticket
-    double2 gacc = make_double2(0.0, 0.0);  // thread 0: running (r.r, r.z) sum of the current group
+    double da = 0.0, rz = 0.0;  // this thread's sums over the current group
     for (uint32_t k = 0;; ++k) {
         const uint32_t s = k % NS, par = (k / NS) & 1u;
         if (lt == 0) s_ok[k & 1u] = mbar_wait(&full[s], par, lim) ? 1 : 0;
@@ -1372,7 +1374,10 @@ __device__ __forceinline__ void upd_consumers(const SysDesc *__restrict__ sys, S
             run_cnt = 0;
         }
         float *stage = smem + s * Lay::kStageFloats;
-        double da = 0.0, rz = 0.0;  // loops: r.r and r.z (r.u); init: b.b and r.z
+        // Loops: r.r and r.z (r.u); init: b.b and r.z; each thread's rows
+        // summed over the current group's tiles (consecutive in this CTA's
+        // walk), so that the FP64 warp and CTA sums run once per group.
+        if (d.gflags & kGroupFirst) da = rz = 0.0;
         const uint32_t *bs = reinterpret_cast<const uint32_t *>(stage + Lay::kBsOff);
         const uint32_t row1 = d.row0 + d.rows;
         // Continuation rows of a long block that started in an earlier tile.
@@ -1385,9 +1390,11 @@ __device__ __forceinline__ void upd_consumers(const SysDesc *__restrict__ sys, S
             const uint32_t end = min(nxt, row1);
             for (uint32_t row = off + 6u; row < end; ++row) passive_row<kK>(d, stage, row, da, rz);
         }
-        da = warp_sum(da);
-        rz = warp_sum(rz);
-        if ((lt & 31u) == 0) wred[lt >> 5] = make_double2(da, rz);
+        const bool closes = (d.gflags & kGroupLast) != 0;
+        if (closes) {
+            const double wa = warp_sum(da), wb = warp_sum(rz);
+            if ((lt & 31u) == 0) wred[lt >> 5] = make_double2(wa, wb);
+        }
         // The consumers wrote their rows into the stage: make those writes
         // visible to the bulk stores below and order them before the bulk
         // loads that will next fill the stage.
@@ -1430,17 +1437,14 @@ __device__ __forceinline__ void upd_consumers(const SysDesc *__restrict__ sys, S
                 }
             }
         }
-        if (lt == 0) {
+        if (lt == 0 && closes) {
             double va = 0.0, vb = 0.0;
 #pragma unroll
             for (int q = 0; q < NU / 32; ++q) {
                 va += wred[q].x;
                 vb += wred[q].y;
             }
-            // A group's tiles come one after another in this CTA's walk: its
-            // partials are added in tile order and stored with its last tile.
-            gacc = (d.gflags & kGroupFirst) ? make_double2(va, vb) : make_double2(gacc.x + va, gacc.y + vb);
-            if (d.gflags & kGroupLast) d.part[d.grp] = gacc;
+            d.part[d.grp] = make_double2(va, vb);
         }
         // The bulk stores have read the stage: hand it back.
         if (lt == kBulkIssuer) bulk_wait_read();
