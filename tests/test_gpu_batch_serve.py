@@ -155,3 +155,44 @@ def test_server_borrowed_inputs_and_device_preparation(ctx, borrow, device_prep)
             assert st["host_prep_ms"] == 0.0
     finally:
         srv.close()
+
+
+def test_server_slot_reuse_while_a_large_request_runs(ctx):
+    """Small requests retire and new ones take their slots while one large
+    request keeps iterating: the engine leaves a stopped system's tiles in
+    its work lists (skipped) until a quarter of the listed tiles have
+    stopped, so a new system in a slot the lists still name must force the
+    lists to be laid out again. Every answer is bit-identical to a solve
+    alone."""
+    import time
+
+    big = wsb.lattice_generate(24, seed=300)
+    smalls = [wsb.lattice_generate(side, seed=310 + i) for i, side in enumerate((4, 5, 3, 6, 4, 5, 3, 4))]
+    srv = wsb.Server(ctx, iters_per_step=4)
+    try:
+        rid_big = srv.submit(big["row_ptr"], big["col_idx"], big["values"], big["block_starts"], big["b"],
+                             max_iter=20000, rel_tol=1e-8)
+        rids, got = [], {}
+        for s in smalls:
+            rid = srv.submit(s["row_ptr"], s["col_idx"], s["values"], s["block_starts"], s["b"], max_iter=5000,
+                             rel_tol=1e-6)
+            rids.append(rid)
+            if len(rids) % 2 == 0:
+                got[rid] = srv.wait(rid, 120.0)  # retired before the next one is submitted
+            else:
+                time.sleep(0.001)
+        res = [got[r] if r in got else srv.wait(r, 120.0) for r in rids]
+        xb, rb = srv.wait(rid_big, 300.0)
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert st["completed"] == len(smalls) + 1
+    for s, (x, r) in zip(smalls, res):
+        m = wsb.Matrix.create(ctx, s["row_ptr"], s["col_idx"], s["values"], s["block_starts"])
+        xa, ra = m.solve(s["b"], max_iter=5000, rel_tol=1e-6)
+        assert r["rc"] == 0 and r["iterations"] == ra["iterations"]
+        assert np.array_equal(x.view(np.uint32), xa.view(np.uint32))
+    m = wsb.Matrix.create(ctx, big["row_ptr"], big["col_idx"], big["values"], big["block_starts"])
+    xa, ra = m.solve(big["b"], max_iter=20000, rel_tol=1e-8)
+    assert rb["rc"] == 0 and rb["iterations"] == ra["iterations"]
+    assert np.array_equal(xb.view(np.uint32), xa.view(np.uint32))
