@@ -341,6 +341,9 @@ static_assert((kColOff * 4) % 16 == 0 && (kBcolOff * 4) % 16 == 0 && (kXgOff * 4
                   (kRpOff * 4) % 16 == 0 && (kSpmvStageFloats * 4) % 128 == 0,
               "TMA alignment");
 static_assert(kSpmvStageFloats >= kRpOff + kSpmvTileRows + 8, "stage size");
+// bsr_stage reads the operands of one block past a tile's last (unused).
+static_assert(36 * (kBsrCapBlocks + 1) <= kXgOff && kXgOff + 6 * (kBsrCapBlocks + 1) <= kSpmvStageFloats,
+              "one block past a tile's last stays inside the stage");
 
 struct SpmvDesc {
     uint32_t valid, sys, tile, layout;
@@ -566,13 +569,15 @@ __device__ __forceinline__ float bsr_stage(const SpmvDesc &d, const float *stage
             const float2 *X = xg + s0 * 3u;
             b0 = B[0], b1 = B[1], b2 = B[2], x0 = X[0], x1 = X[1], x2 = X[2];
         }
+#pragma unroll 2
         for (uint32_t blk = s0; blk < s1; ++blk) {
-            float2 nb0 = b0, nb1 = b1, nb2 = b2, nx0 = x0, nx1 = x1, nx2 = x2;
-            if (blk + 1 < s1) {
-                const float2 *B = reinterpret_cast<const float2 *>(stage + (blk + 1) * 36u + a * 6u);
-                const float2 *X = xg + (blk + 1) * 3u;
-                nb0 = B[0], nb1 = B[1], nb2 = B[2], nx0 = X[0], nx1 = X[1], nx2 = X[2];
-            }
+            // Block blk + 1 <= the tile's block count stays inside the stage
+            // (the block-column and row-pointer areas follow the values and
+            // the gathered x), so it is loaded without a test; past the block
+            // row's end the values are never used.
+            const float2 *B = reinterpret_cast<const float2 *>(stage + (blk + 1) * 36u + a * 6u);
+            const float2 *X = xg + (blk + 1) * 3u;
+            const float2 nb0 = B[0], nb1 = B[1], nb2 = B[2], nx0 = X[0], nx1 = X[1], nx2 = X[2];
             // The six products (packed two at a time), then the adds in
             // index order.
             const float2 q0 = mul2_rn(b0, x0), q1 = mul2_rn(b1, x1), q2 = mul2_rn(b2, x2);
