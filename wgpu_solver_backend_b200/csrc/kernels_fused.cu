@@ -1072,12 +1072,12 @@ constexpr int z_slot() {
 // 93-101, U backward solve dividing by U(i,i) lines 103-122, rows i < m only,
 // lines 79 and 124-126), and writes its rows' new r and z back into the
 // stage. FP64 r.r (init: b.b) and r.z of the rows go to da and rz.
-template <int kK>
+template <int kK, bool kFull>
 __device__ __forceinline__ void bj_block(const UpdDesc &d, float *stage, uint32_t j, double &da, double &rz) {
     using Lay = UpdLayout<kK>;
     const uint32_t *bs = reinterpret_cast<const uint32_t *>(stage + Lay::kBsOff);
     const uint32_t off = bs[d.blk0 + j - d.ba], nxt = bs[d.blk0 + j + 1 - d.ba];
-    const uint32_t m = min(nxt - off, 6u);
+    const uint32_t m = kFull ? 6u : min(nxt - off, 6u);  // kFull: a block of 6 or more rows
     const uint32_t ro = off - d.ra;
     const float2 *L2 = reinterpret_cast<const float2 *>(stage + Lay::kLuOff + j * 36u);
     float L[36];
@@ -1389,9 +1389,13 @@ __device__ __forceinline__ void upd_consumers(const SysDesc *__restrict__ sys, S
         const uint32_t lead_end = d.nblk ? bs[d.blk0 - d.ba] : row1;
         for (uint32_t row = d.row0 + lt; row < lead_end; row += NU) passive_row<kK>(d, stage, row, da, rz);
         if (lt < d.nblk) {
-            bj_block<kK>(d, stage, lt, da, rz);
-            // The block's rows >= 6 inside this tile.
             const uint32_t off = bs[d.blk0 + lt - d.ba], nxt = bs[d.blk0 + lt + 1 - d.ba];
+            // Blocks of 6 or more rows (all of them in a 6-DOF lattice) take a
+            // copy of the solve without the row-count tests (80^3 k_update
+            // 34.9 -> 32.8 us).
+            if (nxt - off >= 6u) bj_block<kK, true>(d, stage, lt, da, rz);
+            else bj_block<kK, false>(d, stage, lt, da, rz);
+            // The block's rows >= 6 inside this tile.
             const uint32_t end = min(nxt, row1);
             for (uint32_t row = off + 6u; row < end; ++row) passive_row<kK>(d, stage, row, da, rz);
         }
